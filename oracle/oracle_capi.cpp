@@ -1,0 +1,334 @@
+// oracle_capi.cpp -- C entry points over gs_oracle.hpp for ctypes.
+//
+// TEST INFRASTRUCTURE ONLY (the parity checker and the CPU baseline); the
+// product never links it.  Layouts follow the reference: params stride 16
+// (shaders.js:14-16), SH channel-major 3K per splat (shaders.js:17-22),
+// proj stride 16 (shaders.js:23-25), gradP stride 16 i32 (shaders.js:26-28).
+#include <cstdio>
+#include <memory>
+
+#include "gs_oracle.hpp"
+
+using namespace gso;
+
+extern "C" {
+
+// Plain-C mirrors of gso::Opts / gso::Cam (field order is the ABI).
+struct OOpts {
+  float eCut, aMin, radClamp, anisoReg;
+  int32_t shDeg, tile;
+  uint64_t entriesCap;
+};
+struct OCam {
+  float R[9];
+  float t[3];
+  float f, cx, cy;
+  int32_t w, h;
+  float gain, bias;
+  uint32_t offset, camIdx, ncams;
+  float activeSh;
+  int32_t train;
+};
+struct OAdam {
+  float lr[16];
+  float b1, b2, eps, bc1, bc2, minLS, maxLS, maxLogit, reg, shLr;
+};
+
+static Opts toOpts(const OOpts* o) {
+  Opts r;
+  r.eCut = o->eCut; r.aMin = o->aMin; r.radClamp = o->radClamp; r.anisoReg = o->anisoReg;
+  r.shDeg = o->shDeg; r.tile = o->tile; r.entriesCap = o->entriesCap;
+  return r;
+}
+static Cam toCam(const OCam* c) {
+  Cam r;
+  for (int k = 0; k < 9; ++k) r.R[k] = c->R[k];
+  for (int k = 0; k < 3; ++k) { r.t[k] = c->t[k]; r.bg[k] = 0.0f; }
+  r.nearz = 0.05f;
+  r.f = c->f; r.cx = c->cx; r.cy = c->cy; r.gain = c->gain;
+  r.W = c->w; r.H = c->h;
+  r.offset = c->offset; r.train = c->train; r.camIdx = c->camIdx; r.ncams = c->ncams;
+  r.bias = c->bias; r.activeSh = c->activeSh;
+  return r;
+}
+static AdamHP toAdam(const OAdam* a) {
+  AdamHP h;
+  for (int k = 0; k < 16; ++k) h.lr[k] = a->lr[k];
+  h.b1 = a->b1; h.b2 = a->b2; h.eps = a->eps; h.bc1 = a->bc1; h.bc2 = a->bc2;
+  h.minLS = a->minLS; h.maxLS = a->maxLS; h.maxLogit = a->maxLogit; h.reg = a->reg; h.shLr = a->shLr;
+  return h;
+}
+
+int oracle_abi_version() { return 1; }
+
+void oracle_adam_bias(double t, float* bc1, float* bc2) { adamBiasCorrection(t, *bc1, *bc2); }
+float oracle_exp_f32(float x) { return exp_f(x); }
+float oracle_log_f32(float x) { return log_f(x); }
+double oracle_sin_f64(double x) { return sin_d(x); }
+float oracle_dither(uint32_t pi) { return ditherOf(pi); }
+
+// ---- pass 1: project (shaders.js:228-315) ----
+void oracle_project_f32(const OOpts* oo, const OCam* oc, const float* params, const float* sh, uint32_t n,
+                        float* proj) {
+  const Opts o = toOpts(oo);
+  const Cam c = toCam(oc);
+  const int K = shRestCoefs(o.shDeg);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < (long)n; ++i)
+    projectOne<float>(o, c, params + (size_t)i * STRIDE, sh ? sh + (size_t)i * 3 * K : nullptr, K,
+                      proj + (size_t)i * STRIDE);
+}
+void oracle_project_f64(const OOpts* oo, const OCam* oc, const double* params, const double* sh, uint32_t n,
+                        double* proj) {
+  const Opts o = toOpts(oo);
+  const Cam c = toCam(oc);
+  const int K = shRestCoefs(o.shDeg);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < (long)n; ++i)
+    projectOne<double>(o, c, params + (size_t)i * STRIDE, sh ? sh + (size_t)i * 3 * K : nullptr, K,
+                       proj + (size_t)i * STRIDE);
+}
+
+// ---- passes 2-4: binning (shaders.js:303-500) ----
+// Writes start[numTiles+1], ids/keys (up to cap entries), per-tile raw
+// counts and drop flags.  Returns the number of kept entries.
+uint64_t oracle_bin_f32(const OOpts* oo, const OCam* oc, const float* proj, uint32_t n, uint32_t* start,
+                        uint32_t* ids, uint32_t* keys, uint64_t cap, uint32_t* cnt, uint8_t* dropped,
+                        uint32_t* overflowTiles) {
+  const Opts o = toOpts(oo);
+  const Cam c = toCam(oc);
+  Bins b = binTiles<float>(o, c, proj, n);
+  std::copy(b.start.begin(), b.start.end(), start);
+  const size_t E = std::min<size_t>(b.ids.size(), cap);
+  std::copy(b.ids.begin(), b.ids.begin() + E, ids);
+  std::copy(b.keys.begin(), b.keys.begin() + E, keys);
+  if (cnt) std::copy(b.cnt.begin(), b.cnt.end(), cnt);
+  if (dropped) std::copy(b.dropped.begin(), b.dropped.end(), dropped);
+  if (overflowTiles) *overflowTiles = b.overflowTiles;
+  return b.ids.size();
+}
+
+static Bins binsFromArrays(const Opts& o, const Cam& c, const uint32_t* start, const uint32_t* ids) {
+  Bins b;
+  b.numTiles = tilesX(c, o.tile) * tilesY(c, o.tile);
+  b.start.assign(start, start + b.numTiles + 1);
+  b.ids.assign(ids, ids + b.start[b.numTiles]);
+  return b;
+}
+
+// ---- render (shaders.js:544-700) on a given binning ----
+void oracle_render_f32(const OOpts* oo, const OCam* oc, const float* proj, const uint32_t* start,
+                       const uint32_t* ids, const uint32_t* targets, float* outImg, float* finalT,
+                       uint32_t* endIdx, int32_t* gradP, uint32_t* stats, int32_t* gradCam, uint64_t* pairs,
+                       int train, int variant) {
+  const Opts o = toOpts(oo);
+  const Cam c = toCam(oc);
+  Bins b = binsFromArrays(o, c, start, ids);
+  std::vector<PixelState> px((size_t)c.W * c.H);
+  AccFixed acc{gradP, stats, gradCam};
+  renderView<float, AccFixed>(o, c, proj, b, targets, outImg, px.data(), acc, train != 0, variant, pairs);
+  for (size_t p = 0; p < px.size(); ++p) {
+    if (finalT) finalT[p] = px[p].T;
+    if (endIdx) endIdx[p] = px[p].end;
+  }
+}
+
+// ---- chain (shaders.js:704-949): consumes and zeroes gradP ----
+void oracle_chain_f32(const OOpts* oo, const OCam* oc, const float* params, const float* proj, const float* sh,
+                      uint32_t n, int32_t* gradP, float* gradF, float* shGrad, int32_t* gradCam) {
+  const Opts o = toOpts(oo);
+  const Cam c = toCam(oc);
+  const int K = shRestCoefs(o.shDeg);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < (long)n; ++i) {
+    float gp[10];
+    int32_t* G = gradP + (size_t)i * STRIDE;
+    for (int k = 0; k < 10; ++k) {
+      const float scale = (k >= 2 && k <= 4) ? FIXEDC : FIXED;
+      gp[k] = (float)G[k] / scale;
+      G[k] = 0;
+    }
+    float shDummy[1];
+    auto camAdd = [&](uint32_t idx, float v) {
+      int32_t q = fixq(v, FIXCAM);
+#pragma omp atomic
+      gradCam[idx] += q;
+    };
+    chainOne<float>(o, c, params + (size_t)i * STRIDE, proj + (size_t)i * STRIDE,
+                    K ? sh + (size_t)i * 3 * K : nullptr, K, gp, gradF + (size_t)i * STRIDE,
+                    K ? shGrad + (size_t)i * 3 * K : shDummy, camAdd);
+  }
+}
+
+// ---- Adam + SH-Adam (shaders.js:952-1036) over n splats ----
+void oracle_adam_f32(const OAdam* oa, uint32_t n, int K, float* params, const float* gradF, float* m, float* v,
+                     float* sh, const float* shGrad, float* shM, float* shV) {
+  const AdamHP h = toAdam(oa);
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < (long)n; ++i) {
+    for (int s = 0; s < STRIDE; ++s) {
+      const size_t j = (size_t)i * STRIDE + s;
+      adamParam(h, s, params[j], gradF[j], m[j], v[j]);
+    }
+    for (int k = 0; k < 3 * K; ++k) {
+      const size_t j = (size_t)i * 3 * K + k;
+      adamSH(h, sh[j], shGrad[j], shM[j], shV[j]);
+    }
+  }
+}
+
+// ---- a whole step over V views: per view project -> bin -> render ->
+// chain, gradients summed over views in view order, then (optionally) Adam.
+// With V = 1 this is stepOnce (trainer.js:398-458).  gradF/shGrad receive
+// the summed gradients when non-null.  Returns 0, or 1 if any view's entry
+// count exceeded entriesCap (the kept entries are still processed).
+int oracle_step_f32(const OOpts* oo, const OCam* cams, int V, const OAdam* oa, uint32_t n, float* params,
+                    float* sh, const uint32_t* targets, float* m, float* v, float* shM, float* shV,
+                    uint32_t* stats, int32_t* gradCam, float* gradF, float* shGrad, int doAdam, int variant,
+                    uint64_t* pairs, float* outImg0) {
+  const Opts o = toOpts(oo);
+  const int K = shRestCoefs(o.shDeg);
+  std::vector<float> gF((size_t)n * STRIDE, 0.0f), sG((size_t)n * 3 * K, 0.0f);
+  std::vector<float> proj((size_t)n * STRIDE), gFv((size_t)n * STRIDE), sGv((size_t)n * 3 * K);
+  std::vector<int32_t> gP((size_t)n * STRIDE, 0);
+  for (int vi = 0; vi < V; ++vi) {
+    const Cam c = toCam(&cams[vi]);
+    oracle_project_f32(oo, &cams[vi], params, K ? sh : nullptr, n, proj.data());
+    Bins b = binTiles<float>(o, c, proj.data(), n);
+    if (stats) stats[3] += b.overflowTiles;
+    std::vector<PixelState> px((size_t)c.W * c.H);
+    std::vector<float> img;
+    if (vi == 0 && outImg0) img.assign((size_t)c.W * c.H * 4, 0.0f);
+    AccFixed acc{gP.data(), stats, gradCam};
+    renderView<float, AccFixed>(o, c, proj.data(), b, targets, img.empty() ? nullptr : img.data(), px.data(), acc,
+                                true, variant, pairs);
+    if (!img.empty()) std::copy(img.begin(), img.end(), outImg0);
+    oracle_chain_f32(oo, &cams[vi], params, proj.data(), K ? sh : nullptr, n, gP.data(), gFv.data(),
+                     K ? sGv.data() : nullptr, gradCam);
+    for (size_t j = 0; j < gF.size(); ++j) gF[j] = gF[j] + gFv[j];
+    for (size_t j = 0; j < sG.size(); ++j) sG[j] = sG[j] + sGv[j];
+  }
+  if (gradF) std::copy(gF.begin(), gF.end(), gradF);
+  if (shGrad && K) std::copy(sG.begin(), sG.end(), shGrad);
+  if (doAdam) oracle_adam_f32(oa, n, K, params, gF.data(), m, v, sh, sG.data(), shM, shV);
+  return 0;
+}
+
+// ---- FP64 host evaluation: loss (Charbonnier sum, squared error, valid
+// px) and unquantised gradients of one view.  gradF/shGrad may be null
+// (loss only, for finite differences). ----
+void oracle_eval_f64(const OOpts* oo, const OCam* oc, const double* params, const double* sh, uint32_t n,
+                     const uint32_t* targets, double* loss3, double* gradF, double* shGrad, float* outImg) {
+  const Opts o = toOpts(oo);
+  const Cam c = toCam(oc);
+  const int K = shRestCoefs(o.shDeg);
+  std::vector<double> proj((size_t)n * STRIDE);
+  oracle_project_f64(oo, oc, params, sh, n, proj.data());
+  Bins b = binTiles<double>(o, c, proj.data(), n);
+  std::vector<double> gP((size_t)n * STRIDE, 0.0), gCam((size_t)(c.ncams + 1) * 8, 0.0);
+  loss3[0] = loss3[1] = loss3[2] = 0.0;
+  AccF64 acc{gP.data(), loss3, gCam.data()};
+  renderView<double, AccF64>(o, c, proj.data(), b, targets, outImg, nullptr, acc, true, 0, nullptr);
+  if (!gradF) return;
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < (long)n; ++i) {
+    double gp[10];
+    for (int k = 0; k < 10; ++k) gp[k] = gP[(size_t)i * STRIDE + k];
+    double shDummy[1];
+    auto camAdd = [](uint32_t, double) {};
+    chainOne<double>(o, c, params + (size_t)i * STRIDE, proj.data() + (size_t)i * STRIDE,
+                     K ? sh + (size_t)i * 3 * K : nullptr, K, gp, gradF + (size_t)i * STRIDE,
+                     (K && shGrad) ? shGrad + (size_t)i * 3 * K : shDummy, camAdd);
+  }
+}
+
+// ---- refine: MCMC-lite relocation + growth (trainer.js:666-794) ----
+// params/m/v are cap*16 f32, sh/shM/shV cap*3K f32.  rng() returns doubles
+// in [0,1) in the order the reference draws them.  JS arithmetic is double;
+// Float32Array stores round to f32, which the casts below reproduce.
+typedef double (*oracle_rng_fn)(void*);
+struct ORefineOut { uint32_t moved, grown, n; int32_t early; };
+
+void oracle_refine(uint32_t n, uint32_t cap, uint32_t growLimit, double iter, double growUntil, double growRate,
+                   int K, float* params, float* m, float* v, float* sh, float* shM, float* shV, oracle_rng_fn rng,
+                   void* ctx, ORefineOut* out) {
+  auto sig = [](double x) { return 1.0 / (1.0 + std::exp(-x)); };
+  std::vector<uint32_t> dead, donors;
+  for (uint32_t i = 0; i < n; ++i) {
+    const double o = sig((double)params[(size_t)i * 16 + 13]);
+    if (o < 0.02) dead.push_back(i);
+    else if (o > 0.4) donors.push_back(i);
+  }
+  out->moved = out->grown = 0; out->n = n; out->early = 0;
+  if (donors.size() < 16) { out->early = 1; return; }
+  const size_t moveCap = (size_t)std::ceil((double)n * 0.05);
+  if (dead.size() > moveCap) dead.resize(moveCap);
+  auto mls = [&](uint32_t i) {
+    const float* p = params + (size_t)i * 16;
+    return ((double)p[3] + (double)p[4] + (double)p[5]) / 3.0;
+  };
+  std::vector<uint32_t> big(donors);
+  std::stable_sort(big.begin(), big.end(), [&](uint32_t a, uint32_t b) { return mls(b) - mls(a) < 0; });
+  big.resize(std::min(big.size(), std::max<size_t>(16, donors.size() >> 2)));
+  const int shr = 3 * K;
+  auto gauss = [&]() {
+    const double u = std::max(1e-9, rng(ctx)), w = rng(ctx);
+    return std::sqrt(-2.0 * std::log(u)) * std::cos(2.0 * M_PI * w);
+  };
+  auto spawnAt = [&](size_t bi, bool allowSplit) {
+    bool doSplit = false;
+    if (allowSplit && big.size() > 16) doSplit = rng(ctx) < 0.7;
+    uint32_t don;
+    if (doSplit) {
+      const size_t di = (size_t)(int32_t)(rng(ctx) * (double)big.size());
+      don = big[di];
+      big[di] = big.back();
+      big.pop_back();
+    } else {
+      don = donors[(size_t)(int32_t)(rng(ctx) * (double)donors.size())];
+    }
+    const size_t bd = (size_t)don * 16;
+    const double s = std::exp(mls(don));
+    for (int k = 0; k < 3; ++k) {
+      const double base = (double)params[bd + k];
+      params[bi + k] = (float)(base + gauss() * s * 0.7);
+    }
+    for (int k = 3; k <= 12; ++k) params[bi + k] = params[bd + k];
+    if (doSplit) {
+      const double shrink = std::log(1.0 / 1.6);
+      for (int k = 3; k <= 5; ++k) {
+        params[bi + k] = (float)((double)params[bi + k] + shrink);
+        params[bd + k] = (float)((double)params[bd + k] + shrink);
+      }
+      params[bi + 13] = params[bd + 13];
+      for (int k = 0; k < 16; ++k) { m[bd + k] = 0.0f; v[bd + k] = 0.0f; }
+    } else {
+      for (int k = 3; k <= 5; ++k) params[bi + k] = (float)((double)params[bi + k] + std::log(0.85));
+      params[bi + 13] = (float)std::log(0.25 / 0.75);
+    }
+    params[bi + 14] = 0.0f; params[bi + 15] = 0.0f;
+    for (int k = 0; k < 16; ++k) { m[bi + k] = 0.0f; v[bi + k] = 0.0f; }
+    if (shr) {
+      const size_t so = (bi / 16) * shr, sd = (size_t)don * shr;
+      for (int k = 0; k < shr; ++k) {
+        sh[so + k] = sh[sd + k];
+        shM[so + k] = 0.0f; shV[so + k] = 0.0f;
+        if (doSplit) { shM[sd + k] = 0.0f; shV[sd + k] = 0.0f; }
+      }
+    }
+  };
+  for (uint32_t i : dead) spawnAt((size_t)i * 16, false);
+  const uint32_t limit = std::min(cap, growLimit ? growLimit : cap);
+  uint32_t grown = 0;
+  if (iter < growUntil) {
+    const double want = std::ceil((double)n * growRate);
+    const double room = (double)limit - (double)n;
+    grown = (uint32_t)std::max(0.0, std::min(want, room));
+  }
+  for (uint32_t k = 0; k < grown; ++k) spawnAt((size_t)(n + k) * 16, true);
+  out->moved = (uint32_t)dead.size();
+  out->grown = grown;
+  out->n = n + grown;
+}
+
+}  // extern "C"
