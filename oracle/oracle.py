@@ -73,6 +73,7 @@ def lib():
         L.oracle_adam_bias.argtypes = [C.c_double, f32p, f32p]
         L.oracle_project_f32.argtypes = [P(OOpts), P(OCam), f32p, f32p, C.c_uint32, f32p]
         L.oracle_project_f64.argtypes = [P(OOpts), P(OCam), f64p, f64p, C.c_uint32, f64p]
+        L.oracle_records_f32.argtypes = [P(OOpts), P(OCam), f32p, C.c_uint32, f32p, u32p]
         L.oracle_bin_f32.restype = C.c_uint64
         L.oracle_bin_f32.argtypes = [P(OOpts), P(OCam), f32p, C.c_uint32, u32p, u32p, u32p, C.c_uint64, u32p,
                                      u8p, u32p]
@@ -132,6 +133,14 @@ def project(o, c, params, sh, n):
     lib().oracle_project_f32(C.byref(o), C.byref(c), _p(params, C.c_float), _p(sh, C.c_float), n,
                              _p(proj, C.c_float))
     return proj
+
+
+def records(o, c, proj, n):
+    rec = np.zeros(n * 12, np.float32)
+    rect = np.zeros(n * 2, np.uint32)
+    lib().oracle_records_f32(C.byref(o), C.byref(c), _p(proj, C.c_float), n, _p(rec, C.c_float),
+                             _p(rect, C.c_uint32))
+    return rec, rect
 
 
 def bin_tiles(o, c, proj, n, cap=None):

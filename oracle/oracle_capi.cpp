@@ -89,6 +89,30 @@ void oracle_project_f64(const OOpts* oo, const OCam* oc, const double* params, c
                        proj + (size_t)i * STRIDE);
 }
 
+// Per-splat values the rasteriser reads, derived from proj exactly as the
+// render pass does (w = opa*comp, cnorm = 1/(1+lambda_max)), plus tile
+// bounds packed {x0 | y0<<16, x1 | y1<<16} ({~0, 0} when culled).
+void oracle_records_f32(const OOpts* oo, const OCam* oc, const float* proj, uint32_t n, float* rec12,
+                        uint32_t* rect2) {
+  const Opts o = toOpts(oo);
+  const Cam c = toCam(oc);
+  for (uint32_t i = 0; i < n; ++i) {
+    const float* pr = proj + (size_t)i * STRIDE;
+    float* r = rec12 + (size_t)i * 12;
+    if (!(pr[11] > 0.0f)) {
+      for (int k = 0; k < 12; ++k) r[k] = 0.0f;
+      rect2[2 * i] = 0xFFFFFFFFu; rect2[2 * i + 1] = 0u;
+      continue;
+    }
+    const Splat2D<float> s = splat2D<float>(pr);
+    const float v[12] = {s.mx, s.my, s.cA, s.cB, s.cC, s.w, s.r, s.g, s.b, s.opa, s.cnorm, pr[2]};
+    for (int k = 0; k < 12; ++k) r[k] = v[k];
+    const TileRect t = tileRect<float>(c, o.tile, pr[0], pr[1], pr[15]);
+    rect2[2 * i] = (uint32_t)t.x0 | ((uint32_t)t.y0 << 16);
+    rect2[2 * i + 1] = (uint32_t)t.x1 | ((uint32_t)t.y1 << 16);
+  }
+}
+
 // ---- passes 2-4: binning (shaders.js:303-500) ----
 // Writes start[numTiles+1], ids/keys (up to cap entries), per-tile raw
 // counts and drop flags.  Returns the number of kept entries.

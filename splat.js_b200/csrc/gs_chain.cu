@@ -1,0 +1,369 @@
+// gs_chain.cu -- per-splat pass after the rasteriser: the chain rule from
+// screen-space gradients to parameter gradients (shaders.js:704-949), fused
+// with Adam (shaders.js:984-1036) and SH-Adam (shaders.js:952-982).
+//
+// One thread per splat.  For a batch of V views, each view's fixed-point
+// screen-space gradients are decoded (and cleared for the next step), chained
+// through that view's camera, and the parameter gradients summed in view
+// order; Adam then updates the splat once.  The reference runs chain, Adam
+// and SH-Adam as three dispatches with gradF / shGrad round-tripping through
+// memory; here they stay in registers unless the caller asks for them
+// (gradient readout for checks).  Operation order follows the WGSL.
+#include "gs_geom.cuh"
+#include "gs_kernels.h"
+
+namespace gs {
+
+struct CamGrad7 {
+  float w[3], t[3], logf;
+};
+
+// chain for one visible splat in one view; gp = decoded screen-space grads
+template <int DEG>
+__device__ __forceinline__ void chainOne(const DevCam& c, const float* P, const Geom& g, float gp[10],
+                                         const float* sh, float anisoReg, float gF[16], float* shG,
+                                         CamGrad7& cg) {
+  constexpr int K = DEG > 0 ? (DEG + 1) * (DEG + 1) - 1 : 0;
+  const float f = c.f, z = g.pc[2], iz = 1.0f / z;
+  // conic -> dilated 2D covariance (shaders.js:758-777)
+  const float ad = g.va + 0.3f, cd = g.vc + 0.3f;
+  const float detVd = ad * cd - g.vb * g.vb;
+  const float inv = 1.0f / detVd;
+  const float kA = cd * inv, kB = -g.vb * inv, kC = ad * inv;
+  const float g11 = gp[2], g12 = 0.5f * gp[3], g22 = gp[4];
+  const float m100 = g11 * kA + g12 * kB, m101 = g11 * kB + g12 * kC;
+  const float m110 = g12 * kA + g22 * kB, m111 = g12 * kB + g22 * kC;
+  const float p00 = kA * m100 + kB * m110, p01 = kA * m101 + kB * m111;
+  const float p10 = kB * m100 + kC * m110, p11 = kB * m101 + kC * m111;
+  float gva = -p00, gvb = -(p01 + p10), gvc = -p11;
+  // comp -> raw 2D covariance (shaders.js:779-788)
+  const float detV = fmaxf(g.va * g.vc - g.vb * g.vb, 0.0f);
+  const float comp = sqrtf(fmaxf(detV / detVd, 0.0f));
+  if (comp > 1e-4f) {
+    const float gcomp = gp[5];
+    const float denom = 2.0f * comp * detVd;
+    gva = gva + gcomp * (g.vc - comp * comp * cd) / denom;
+    gvc = gvc + gcomp * (g.va - comp * comp * ad) / denom;
+    gvb = gvb + gcomp * (2.0f * g.vb * (comp * comp - 1.0f)) / denom;
+  }
+  // V = T Sigma T^T backward (shaders.js:790-810)
+  const float h11 = gva, h12 = 0.5f * gvb, h22 = gvc;
+  float u0[3], u1[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    u0[k] = h11 * g.t0[k] + h12 * g.t1[k];
+    u1[k] = h12 * g.t0[k] + h22 * g.t1[k];
+  }
+  const float* t0 = g.t0;
+  const float* t1 = g.t1;
+  const float dS00 = t0[0] * u0[0] + t1[0] * u1[0];
+  const float dS01 = 0.5f * ((t0[0] * u0[1] + t1[0] * u1[1]) + (t0[1] * u0[0] + t1[1] * u1[0]));
+  const float dS02 = 0.5f * ((t0[0] * u0[2] + t1[0] * u1[2]) + (t0[2] * u0[0] + t1[2] * u1[0]));
+  const float dS11 = t0[1] * u0[1] + t1[1] * u1[1];
+  const float dS12 = 0.5f * ((t0[1] * u0[2] + t1[1] * u1[2]) + (t0[2] * u0[1] + t1[2] * u1[1]));
+  const float dS22 = t0[2] * u0[2] + t1[2] * u1[2];
+  const float sT0[3] = {g.s00 * t0[0] + g.s01 * t0[1] + g.s02 * t0[2],
+                        g.s01 * t0[0] + g.s11 * t0[1] + g.s12 * t0[2],
+                        g.s02 * t0[0] + g.s12 * t0[1] + g.s22 * t0[2]};
+  const float sT1[3] = {g.s00 * t1[0] + g.s01 * t1[1] + g.s02 * t1[2],
+                        g.s01 * t1[0] + g.s11 * t1[1] + g.s12 * t1[2],
+                        g.s02 * t1[0] + g.s12 * t1[1] + g.s22 * t1[2]};
+  float dT0[3], dT1[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    dT0[k] = 2.0f * (h11 * sT0[k] + h12 * sT1[k]);
+    dT1[k] = 2.0f * (h12 * sT0[k] + h22 * sT1[k]);
+  }
+  // T = J W: position through J (shaders.js:812-822)
+  const float R0[3] = {c.R[0], c.R[1], c.R[2]};
+  const float R1[3] = {c.R[3], c.R[4], c.R[5]};
+  const float R2[3] = {c.R[6], c.R[7], c.R[8]};
+  const float dJ00 = dot3(dT0, R0), dJ02 = dot3(dT0, R2), dJ11 = dot3(dT1, R1), dJ12 = dot3(dT1, R2);
+  float dpc[3] = {0.0f, 0.0f, 0.0f};
+  dpc[0] = dpc[0] + dJ02 * ((-f) * iz * iz);
+  dpc[1] = dpc[1] + dJ12 * ((-f) * iz * iz);
+  dpc[2] = dpc[2] + ((dJ00 + dJ11) * ((-f) * iz * iz) + dJ02 * (2.0f * f * g.pc[0] * iz * iz * iz) +
+                     dJ12 * (2.0f * f * g.pc[1] * iz * iz * iz));
+  // mean path (shaders.js:824-827)
+  dpc[0] = dpc[0] + gp[0] * f * iz;
+  dpc[1] = dpc[1] + gp[1] * f * iz;
+  dpc[2] = dpc[2] + (-f) * (gp[0] * g.pc[0] + gp[1] * g.pc[1]) * iz * iz;
+  // W^T dpc (shaders.js:830-832)
+  gF[0] = R0[0] * dpc[0] + R1[0] * dpc[1] + R2[0] * dpc[2];
+  gF[1] = R0[1] * dpc[0] + R1[1] * dpc[1] + R2[1] * dpc[2];
+  gF[2] = R0[2] * dpc[0] + R1[2] * dpc[1] + R2[2] * dpc[2];
+  // camera pose gradients (shaders.js:835-858)
+  if (c.train) {
+    cg.t[0] = dpc[0]; cg.t[1] = dpc[1]; cg.t[2] = dpc[2];
+    const float pt[3] = {g.pc[0] - c.t[0], g.pc[1] - c.t[1], g.pc[2] - c.t[2]};
+    float dw[3] = {pt[1] * dpc[2] - pt[2] * dpc[1], pt[2] * dpc[0] - pt[0] * dpc[2],
+                   pt[0] * dpc[1] - pt[1] * dpc[0]};
+    float dW0[3], dW1[3], dW2[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      dW0[k] = (f * iz) * dT0[k];
+      dW1[k] = (f * iz) * dT1[k];
+      dW2[k] = ((-f) * g.pc[0] * iz * iz) * dT0[k] + ((-f) * g.pc[1] * iz * iz) * dT1[k];
+    }
+    float acc3[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float wc[3] = {c.R[k], c.R[3 + k], c.R[6 + k]};
+      const float vv[3] = {dW0[k], dW1[k], dW2[k]};
+      const float cr[3] = {wc[1] * vv[2] - wc[2] * vv[1], wc[2] * vv[0] - wc[0] * vv[2],
+                           wc[0] * vv[1] - wc[1] * vv[0]};
+      if (k == 0) { acc3[0] = cr[0]; acc3[1] = cr[1]; acc3[2] = cr[2]; }
+      else { acc3[0] = acc3[0] + cr[0]; acc3[1] = acc3[1] + cr[1]; acc3[2] = acc3[2] + cr[2]; }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cg.w[k] = dw[k] + acc3[k];
+    cg.logf = gp[0] * f * g.pc[0] * iz + gp[1] * f * g.pc[1] * iz + (dJ00 + dJ11) * (f * iz) +
+              dJ02 * ((-f) * g.pc[0] * iz * iz) + dJ12 * ((-f) * g.pc[1] * iz * iz);
+  }
+  // Sigma = M M^T backward -> scales (shaders.js:860-884)
+  float m0[3], m1[3], m2[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    m0[k] = g.r0[k] * g.s[k];
+    m1[k] = g.r1[k] * g.s[k];
+    m2[k] = g.r2[k] * g.s[k];
+  }
+  float dM0[3], dM1[3], dM2[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    dM0[k] = 2.0f * (dS00 * m0[k] + dS01 * m1[k] + dS02 * m2[k]);
+    dM1[k] = 2.0f * (dS01 * m0[k] + dS11 * m1[k] + dS12 * m2[k]);
+    dM2[k] = 2.0f * (dS02 * m0[k] + dS12 * m1[k] + dS22 * m2[k]);
+  }
+  float dsv[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) dsv[k] = dM0[k] * g.r0[k] + dM1[k] * g.r1[k] + dM2[k] * g.r2[k];
+  const float ls[3] = {clampf(P[3], -12.0f, 6.0f), clampf(P[4], -12.0f, 6.0f), clampf(P[5], -12.0f, 6.0f)};
+  const float mls = (ls[0] + ls[1] + ls[2]) / 3.0f;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) gF[3 + k] = dsv[k] * g.s[k] + anisoReg * (ls[k] - mls);
+  // quaternion backward (shaders.js:886-904)
+  float dR0[3], dR1[3], dR2[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    dR0[k] = dM0[k] * g.s[k];
+    dR1[k] = dM1[k] * g.s[k];
+    dR2[k] = dM2[k] * g.s[k];
+  }
+  const float qw = g.q[0], qx = g.q[1], qy = g.q[2], qz = g.q[3];
+  const float gw = 2.0f * (dR0[1] * (-qz) + dR0[2] * qy + dR1[0] * qz + dR1[2] * (-qx) + dR2[0] * (-qy) +
+                           dR2[1] * qx);
+  const float gx = 2.0f * (dR0[1] * qy + dR0[2] * qz + dR1[0] * qy + dR1[1] * (-2.0f * qx) + dR1[2] * (-qw) +
+                           dR2[0] * qz + dR2[1] * qw + dR2[2] * (-2.0f * qx));
+  const float gy = 2.0f * (dR0[0] * (-2.0f * qy) + dR0[1] * qx + dR0[2] * qw + dR1[0] * qx + dR1[2] * qz +
+                           dR2[0] * (-qw) + dR2[1] * qz + dR2[2] * (-2.0f * qy));
+  const float gz = 2.0f * (dR0[0] * (-2.0f * qz) + dR0[1] * (-qw) + dR0[2] * qx + dR1[0] * qw +
+                           dR1[1] * (-2.0f * qz) + dR1[2] * qy + dR2[0] * qx + dR2[1] * qy);
+  const float gq[4] = {gw, gx, gy, gz};
+  const float ql = fmaxf(sqrtf(P[6] * P[6] + P[7] * P[7] + P[8] * P[8] + P[9] * P[9]), 1e-6f);
+  const float qd = g.q[0] * gq[0] + g.q[1] * gq[1] + g.q[2] * gq[2] + g.q[3] * gq[3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) gF[6 + k] = (gq[k] - g.q[k] * qd) / ql;
+  // colour: DC sigmoid chain + SH bands (+ position via view dir) (shaders.js:906-947)
+  const float sCol[3] = {sigm(P[10]), sigm(P[11]), sigm(P[12])};
+  float dRGB[3] = {gp[7], gp[8], gp[9]};
+  if (K > 0) {
+    float cp[3];
+    camPosWorld(c, cp);
+    const float un[3] = {P[0] - cp[0], P[1] - cp[1], P[2] - cp[2]};
+    const float ulen = fmaxf(sqrtf(dot3(un, un)), 1e-9f);
+    const float vd[3] = {un[0] / ulen, un[1] / ulen, un[2] / ulen};
+    float Y[15], D[15][3];
+    shBasis<DEG>(vd, Y);
+    shBasisGrad<DEG>(vd, D);
+    const int aK = shActiveK(c, K);
+    float col[3] = {sCol[0], sCol[1], sCol[2]};
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (k < aK) {
+        col[0] = col[0] + sh[k] * Y[k];
+        col[1] = col[1] + sh[K + k] * Y[k];
+        col[2] = col[2] + sh[2 * K + k] * Y[k];
+      }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) dRGB[j] = dRGB[j] * (col[j] > 0.0f ? 1.0f : 0.0f);
+    float gv[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (k < aK) {
+        shG[k] = dRGB[0] * Y[k];
+        shG[K + k] = dRGB[1] * Y[k];
+        shG[2 * K + k] = dRGB[2] * Y[k];
+        const float wk = dRGB[0] * sh[k] + dRGB[1] * sh[K + k] + dRGB[2] * sh[2 * K + k];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) gv[j] = gv[j] + wk * D[k][j];
+      }
+    const float vg = dot3(vd, gv);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) gF[j] = gF[j] + (gv[j] - vd[j] * vg) / ulen;
+  }
+#pragma unroll
+  for (int j = 0; j < 3; ++j) gF[10 + j] = dRGB[j] * sCol[j] * (1.0f - sCol[j]);
+  gF[13] = gp[6];
+}
+
+__device__ __forceinline__ void adamParam(const AdamHP& h, int slot, float& p, float g, float& m, float& v) {
+  const float lr = h.lr[slot];
+  if (lr == 0.0f) return;
+  if (!(fabsf(g) < 1e18f)) g = 0.0f;
+  if (slot == 13) {
+    const float sg = sigm(p);
+    g = g + h.reg * sg * (1.0f - sg);
+  }
+  m = h.b1 * m + (1.0f - h.b1) * g;
+  v = h.b2 * v + (1.0f - h.b2) * g * g;
+  const float mh = m / h.bc1, vh = v / h.bc2;
+  float pn = p - h.lr[slot] * mh / (sqrtf(vh) + h.eps);
+  if (slot >= 3 && slot <= 5) pn = clampf(pn, h.minLS, h.maxLS);
+  if (slot >= 10 && slot <= 13) pn = clampf(pn, -h.maxLogit, h.maxLogit);
+  p = pn;
+}
+
+template <int DEG>
+__global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
+  constexpr int K = DEG > 0 ? (DEG + 1) * (DEG + 1) - 1 : 0;
+  constexpr int SHN = 3 * K > 0 ? 3 * K : 1;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = i < a.n;
+  const int lane = threadIdx.x & 31;
+
+  float P[16];
+  float sh[SHN];
+  float gFa[16];
+  float shA[SHN];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) { P[k] = 0.0f; gFa[k] = 0.0f; }
+#pragma unroll
+  for (int k = 0; k < SHN; ++k) { sh[k] = 0.0f; shA[k] = 0.0f; }
+  if (valid) {
+    const float4* P4 = reinterpret_cast<const float4*>(a.params + (size_t)i * STRIDE);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float4 t = P4[k];
+      P[4 * k] = t.x; P[4 * k + 1] = t.y; P[4 * k + 2] = t.z; P[4 * k + 3] = t.w;
+    }
+    if (K > 0) {
+      const float* s = a.sh + (size_t)i * 3 * K;
+#pragma unroll
+      for (int k = 0; k < 3 * K; ++k) sh[k] = s[k];
+    }
+  }
+
+  for (int v = 0; v < a.V; ++v) {
+    const DevCam& c = a.cams[v];
+    float gF[16];
+    float shG[SHN];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) gF[k] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < SHN; ++k) shG[k] = 0.0f;
+    CamGrad7 cg = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f};
+    if (valid) {
+      const size_t slot = (size_t)v * a.n + i;
+      int4* G4 = reinterpret_cast<int4*>(a.gradP + slot * GP_STRIDE);
+      const int4 q0 = G4[0], q1 = G4[1], q2 = G4[2];
+      G4[0] = make_int4(0, 0, 0, 0);
+      G4[1] = make_int4(0, 0, 0, 0);
+      G4[2] = make_int4(0, 0, 0, 0);
+      const int32_t qi[10] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y};
+      float gp[10];
+#pragma unroll
+      for (int k = 0; k < 10; ++k) gp[k] = (float)qi[k] / ((k >= 2 && k <= 4) ? FIXEDC : FIXED);
+      if (a.rect[slot].x != 0xFFFFFFFFu) {
+        const Geom g = computeGeom(c, P);
+        if (g.ok) {
+          // undo the render pass's conic normalisation (shaders.js:735-744)
+          const float cva = g.va + 0.3f, cvc = g.vc + 0.3f;
+          const float cmid = 0.5f * (cva + cvc);
+          const float lmax = cmid + sqrtf(fmaxf(cmid * cmid - (cva * cvc - g.vb * g.vb), 0.0f));
+          const float cden = 1.0f + lmax;
+          gp[2] = gp[2] * cden; gp[3] = gp[3] * cden; gp[4] = gp[4] * cden;
+          chainOne<DEG>(c, P, g, gp, sh, a.anisoReg, gF, shG, cg);
+        }
+      }
+    }
+    // camera gradients: warp sums of the fixed-point values, one atomic each
+    if (c.train) {
+      const float cv[7] = {cg.w[0], cg.w[1], cg.w[2], cg.t[0], cg.t[1], cg.t[2], cg.logf};
+#pragma unroll
+      for (int k = 0; k < 7; ++k) {
+        const uint32_t r = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)fixq(cv[k], FIXCAM));
+        if (lane == 0 && r) {
+          const uint32_t idx = k < 6 ? c.camIdx * 8u + (uint32_t)k : c.ncams * 8u;
+          atomicAdd(&a.gradCam[idx], (int32_t)r);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) gFa[k] = gFa[k] + gF[k];
+#pragma unroll
+    for (int k = 0; k < SHN; ++k) shA[k] = shA[k] + shG[k];
+  }
+  if (!valid) return;
+  if (a.gradF) {
+    float4* o = reinterpret_cast<float4*>(a.gradF + (size_t)i * STRIDE);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o[k] = make_float4(gFa[4 * k], gFa[4 * k + 1], gFa[4 * k + 2], gFa[4 * k + 3]);
+    if (K > 0) {
+      float* so = a.shGrad + (size_t)i * 3 * K;
+#pragma unroll
+      for (int k = 0; k < 3 * K; ++k) so[k] = shA[k];
+    }
+  }
+  if (!a.doAdam) return;
+  float4* M4 = reinterpret_cast<float4*>(a.m + (size_t)i * STRIDE);
+  float4* V4 = reinterpret_cast<float4*>(a.v + (size_t)i * STRIDE);
+  float m[16], vv[16];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float4 mm = M4[k], vq = V4[k];
+    m[4 * k] = mm.x; m[4 * k + 1] = mm.y; m[4 * k + 2] = mm.z; m[4 * k + 3] = mm.w;
+    vv[4 * k] = vq.x; vv[4 * k + 1] = vq.y; vv[4 * k + 2] = vq.z; vv[4 * k + 3] = vq.w;
+  }
+#pragma unroll
+  const AdamHP hpv = *a.hp;
+#pragma unroll
+  for (int s = 0; s < 16; ++s) adamParam(hpv, s, P[s], gFa[s], m[s], vv[s]);
+  float4* P4o = reinterpret_cast<float4*>(a.params + (size_t)i * STRIDE);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    P4o[k] = make_float4(P[4 * k], P[4 * k + 1], P[4 * k + 2], P[4 * k + 3]);
+    M4[k] = make_float4(m[4 * k], m[4 * k + 1], m[4 * k + 2], m[4 * k + 3]);
+    V4[k] = make_float4(vv[4 * k], vv[4 * k + 1], vv[4 * k + 2], vv[4 * k + 3]);
+  }
+  if (K > 0) {
+    float* shp = a.sh + (size_t)i * 3 * K;
+    float* shm = a.shM + (size_t)i * 3 * K;
+    float* shv = a.shV + (size_t)i * 3 * K;
+    const AdamHP& h = hpv;
+#pragma unroll
+    for (int k = 0; k < 3 * K; ++k) {
+      float g = shA[k];
+      if (!(fabsf(g) < 1e18f)) g = 0.0f;
+      const float mk = h.b1 * shm[k] + (1.0f - h.b1) * g;
+      const float vk = h.b2 * shv[k] + (1.0f - h.b2) * g * g;
+      shm[k] = mk;
+      shv[k] = vk;
+      const float mh = mk / h.bc1, vh = vk / h.bc2;
+      shp[k] = sh[k] - h.shLr * mh / (sqrtf(vh) + h.eps);
+    }
+  }
+}
+
+void launch_chain_adam(const ChainArgs& a, int deg, cudaStream_t s) {
+  const unsigned grid = (a.n + 127) / 128;
+  if (grid == 0) return;
+  switch (deg) {
+    case 0: k_chain_adam<0><<<grid, 128, 0, s>>>(a); break;
+    case 1: k_chain_adam<1><<<grid, 128, 0, s>>>(a); break;
+    case 2: k_chain_adam<2><<<grid, 128, 0, s>>>(a); break;
+    default: k_chain_adam<3><<<grid, 128, 0, s>>>(a); break;
+  }
+}
+
+}  // namespace gs

@@ -1,0 +1,159 @@
+// gs_common.cuh -- device-side conventions shared by every kernel.
+//
+// Numerics.  The library is compiled with -fmad=false: no a*b+c is fused
+// unless the source writes fmaf().  Division and square root are IEEE
+// (-prec-div/-prec-sqrt default), denormals are kept (no -ftz).  exp, log and
+// the dither's sin are computed by the canonical functions below (written
+// from the mathematics, not from any library), so every FP32 value a kernel
+// produces is reproducible bit for bit by a host restatement that performs
+// the same operations.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gs {
+
+constexpr int STRIDE = 16;          // params / proj stride (shaders.js:14-25)
+constexpr int GP_STRIDE = 12;       // screen-space gradient slots 0-9 (+2 pad) per splat
+constexpr float FIXED = 16384.0f;   // shaders.js:35
+constexpr float FIXEDC = 16384.0f;  // shaders.js:39
+constexpr float FIXCAM = 64.0f;     // shaders.js:158
+constexpr uint32_t SHSORT = 2048;   // shaders.js:33 (padding rule of the entry budget)
+constexpr int MAX_K = 15;           // SH rest coefficients per channel at degree 3
+
+// Device camera record: the Cam uniform of shaders.js:140-152 as
+// _camUniform fills it (trainer.js:357-372), plus derived tile geometry.
+struct DevCam {
+  float R[9];
+  float t[3];
+  float nearz;
+  float f, cx, cy, gain;
+  float bg[3];
+  float bias;
+  float activeSh;
+  int32_t W, H;
+  int32_t tilesX, tilesY;
+  uint32_t offset;     // pixel offset of this view's target image
+  uint32_t camIdx;     // gradCam row
+  uint32_t ncams;      // gradCam focal row index
+  int32_t train;
+  uint32_t tileBase;   // first global tile id of this view in a batch
+  uint32_t pixBase;    // first pixel of this view in the batch's pixel buffers
+};
+
+// Per-(view, splat) record read by the rasteriser: 3 x float4 = 48 B.
+//   r0 = (mx, my, cA, cB)  r1 = (cC, w = opa*comp, r, g)  r2 = (b, opa, cnorm, depth)
+struct __align__(16) RenderRec {
+  float4 r0, r1, r2;
+};
+
+// ---- canonical scalar functions --------------------------------------------
+// exp(x), |x| <= 87: Cody-Waite reduction x = k ln2 + r with ln2 split in a
+// 16-bit head and a tail, e^r by its degree-7 Taylor series on
+// |r| <= ln2/2, times 2^k assembled from the rounding constant's bits.
+__device__ __forceinline__ float gexp(float x) {
+  const float RND = 12582912.0f;  // 1.5 * 2^23
+  float t = __fmaf_rn(x, 1.44269504088896341f, RND);
+  float k = __fsub_rn(t, RND);
+  float r = __fmaf_rn(k, -0.693145751953125f, x);
+  r = __fmaf_rn(k, -1.42860676533018700e-6f, r);
+  float p = 1.98412698412698413e-4f;
+  p = __fmaf_rn(p, r, 1.38888888888888889e-3f);
+  p = __fmaf_rn(p, r, 8.33333333333333333e-3f);
+  p = __fmaf_rn(p, r, 4.16666666666666667e-2f);
+  p = __fmaf_rn(p, r, 1.66666666666666667e-1f);
+  p = __fmaf_rn(p, r, 0.5f);
+  p = __fmaf_rn(p, r, 1.0f);
+  p = __fmaf_rn(p, r, 1.0f);
+  uint32_t sb = (__float_as_uint(t) << 23) + 0x3F800000u;
+  return __fmul_rn(p, __uint_as_float(sb));
+}
+
+// log(x), x positive normal: x = m 2^e, m in [sqrt(1/2), sqrt(2)),
+// log m = 2 atanh((m-1)/(m+1)) by its odd series to degree 11.
+__device__ __forceinline__ float glog(float x) {
+  uint32_t b = __float_as_uint(x);
+  int e = (int)((b >> 23) & 0xFFu) - 127;
+  float m = __uint_as_float((b & 0x7FFFFFu) | 0x3F800000u);
+  if (m > 1.41421356f) { m = m * 0.5f; e += 1; }
+  float s = __fdiv_rn(m - 1.0f, m + 1.0f);
+  float s2 = s * s;
+  float p = 9.09090909090909091e-2f;
+  p = __fmaf_rn(p, s2, 1.11111111111111111e-1f);
+  p = __fmaf_rn(p, s2, 1.42857142857142857e-1f);
+  p = __fmaf_rn(p, s2, 2.00000000000000000e-1f);
+  p = __fmaf_rn(p, s2, 3.33333333333333333e-1f);
+  p = __fmaf_rn(p, s2, 1.0f);
+  float lm = (s + s) * p;
+  float fe = (float)e;
+  return __fmaf_rn(fe, 0.693145751953125f, __fmaf_rn(fe, 1.42860676533018700e-6f, lm));
+}
+
+// sin(x) in double, |x| < 2^31: quadrant reduction by pi/2 (28-bit head so
+// k * head is exact, plus a tail), Taylor series of sin/cos on |r| <= pi/4.
+__device__ __forceinline__ double gsin_d(double x) {
+  const double PIO2_HI = 1.570796325802803;
+  const double PIO2_LO = 9.920935796805404e-10;
+  double k = rint(__dmul_rn(x, 0.6366197723675814));
+  double r = __dsub_rn(__dsub_rn(x, __dmul_rn(k, PIO2_HI)), __dmul_rn(k, PIO2_LO));
+  long long q = ((long long)k) & 3;
+  double r2 = r * r;
+  double s = 2.8114572543455206e-15;
+  s = s * r2 - 7.647163731819816e-13;
+  s = s * r2 + 1.6059043836821613e-10;
+  s = s * r2 - 2.505210838544172e-08;
+  s = s * r2 + 2.7557319223985893e-06;
+  s = s * r2 - 1.984126984126984e-04;
+  s = s * r2 + 8.333333333333333e-03;
+  s = s * r2 - 1.6666666666666666e-01;
+  s = (s * r2) * r + r;
+  double c = 1.5619206968586225e-16;
+  c = c * r2 - 4.779477332387385e-14;
+  c = c * r2 + 1.1470745597729725e-11;
+  c = c * r2 - 2.08767569878681e-09;
+  c = c * r2 + 2.755731922398589e-07;
+  c = c * r2 - 2.48015873015873e-05;
+  c = c * r2 + 1.388888888888889e-03;
+  c = c * r2 - 4.1666666666666664e-02;
+  c = c * r2 + 0.5;
+  c = 1.0 - c * r2;
+  if (q == 0) return s;
+  if (q == 1) return c;
+  if (q == 2) return -s;
+  return -c;
+}
+
+__device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+// 1 / (1 + exp(-clamp(x, -9, 9)))
+__device__ __forceinline__ float sigm(float x) { return 1.0f / (1.0f + gexp(-clampf(x, -9.0f, 9.0f))); }
+// i32(clamp(v * scale, -1e9, 1e9)) with WGSL's truncating cast (shaders.js:529-541)
+__device__ __forceinline__ int32_t fixq(float v, float scale) {
+  float s = v * scale;
+  s = fminf(fmaxf(s, -1.0e9f), 1.0e9f);
+  return __float2int_rz(s);
+}
+// u32(f32): truncate, saturate, NaN -> 0
+__device__ __forceinline__ uint32_t u32sat(float x) { return __float2uint_rz(x); }
+
+// fract(sin(f32(pi) * 12.9898) * 43758.5453): the PSNR dither (shaders.js:605)
+__device__ __forceinline__ float dither(uint32_t pi) {
+  float a = (float)pi * 12.9898f;
+  float s = (float)gsin_d((double)a);
+  float v = s * 43758.5453f;
+  return v - floorf(v);
+}
+
+__device__ __forceinline__ int shActiveK(const DevCam& c, int K) {
+  uint32_t ad = u32sat(c.activeSh + 0.5f);
+  uint32_t k = (ad + 1u) * (ad + 1u) - 1u;
+  return (int)min(k, (uint32_t)K);
+}
+
+// Status flags shared with the host (device status word, bit set).
+enum StatusBits : uint32_t {
+  ST_LOOKBACK_TIMEOUT = 1u << 0,  // a decoupled look-back spin reached its limit
+  ST_ENTRY_OVERFLOW = 1u << 1,    // more (tile, splat) entries than the entry buffer holds
+  ST_BAD_INPUT = 1u << 2,
+};
+
+}  // namespace gs

@@ -1,0 +1,193 @@
+// gs_kernels.h -- launch arguments of the training-step kernels (host and
+// device share these plain structs; nothing here is part of the C ABI).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gs_common.cuh"
+
+namespace gs {
+
+struct ProjectArgs {
+  const float* params;     // n * 16
+  const float* sh;         // n * 3K (channel-major) or null
+  uint32_t n;
+  int V;
+  const DevCam* cams;      // V views
+  float eCut, aMin, radClamp;
+  int tile;
+  RenderRec* recs;         // V * n
+  uint2* rect;             // V * n
+  int32_t* diffGrid;       // per view (tilesX+1)*(tilesY+1), cleared before
+  const uint32_t* gridBase;  // V offsets into diffGrid
+};
+
+struct TileRangeArgs {
+  int V;
+  const DevCam* cams;
+  int32_t* diffGrid;
+  const uint32_t* gridBase;
+  uint32_t* tileCnt;       // per global tile: the reference's tileCnt
+  uint8_t* dropped;        // per global tile: dropped by the entry budget
+  uint2* ranges;           // per global tile: [start, end) in the sorted entries
+  uint32_t* viewDrops;     // per view: number of dropped tiles
+  uint32_t* stats;         // stats[3] += dropped tiles
+  uint64_t entriesCap;     // per-view entry budget (ENTCAP)
+  uint32_t* totalEntries;  // out: kept entries over the batch
+};
+
+struct SplatCountArgs {
+  uint32_t n;
+  int V;
+  const DevCam* cams;
+  const uint2* rect;
+  const uint8_t* dropped;
+  const uint32_t* viewDrops;
+  uint32_t* counts;        // V * n
+};
+
+struct KeygenArgs {
+  uint32_t n;
+  int V;
+  const DevCam* cams;
+  const uint2* rect;
+  const RenderRec* recs;
+  const uint8_t* dropped;
+  const uint32_t* viewDrops;
+  const uint32_t* offsets;  // V * n exclusive scan of counts
+  uint64_t* keys;
+  uint32_t* vals;
+  uint64_t capacity;
+  uint32_t* status;
+};
+
+struct RadixHistArgs {
+  const uint64_t* keys;
+  const uint32_t* nItems;
+  uint32_t* hist;           // passes * 256
+  int passes;
+  uint32_t* epoch;
+};
+
+struct OnesweepArgs {
+  const uint64_t* keysIn;
+  const uint32_t* valsIn;
+  uint64_t* keysOut;        // null: do not write keys (last pass)
+  uint32_t* valsOut;
+  const uint32_t* nItems;
+  const uint32_t* hist;
+  uint32_t* tileCounter;    // per pass
+  uint64_t* status;         // look-back words, one per (block, digit)
+  uint32_t* statusWord;     // error bits
+  const uint32_t* epoch;
+  int pass;
+};
+
+struct RadixSortArgs {
+  uint64_t* keys[2];
+  uint32_t* vals[2];
+  const uint32_t* nItems;
+  uint32_t* hist;
+  uint32_t* tileCounter;
+  uint64_t* status;
+  uint32_t* statusWord;
+  uint32_t* epoch;
+  int passes;
+  bool keepKeys;
+  unsigned histGrid, sweepGrid;
+};
+
+struct RasterArgs {
+  const DevCam* cams;
+  int V;
+  uint32_t n;
+  const RenderRec* recs;   // V * n
+  const uint32_t* ids;     // sorted entry values (splat ids)
+  const uint2* ranges;     // per global tile
+  uint32_t totalTiles;
+  const uint32_t* workOrder;  // null: item order
+  uint32_t* workCounter;      // null: one item per block (blockIdx.x)
+  float eCut, aMin;
+  float4* outImg;          // per batch pixel (RGB, 1 - T)
+  float* finalT;
+  uint32_t* endIdx;
+  const uint32_t* targets;
+  int32_t* gradP;          // V * n * GP_STRIDE
+  uint32_t* stats;
+  int32_t* gradCam;
+  float* tStore;           // stored-state variant: T before each entry, per pixel
+};
+
+struct AdamHP {
+  float lr[16];
+  float b1, b2, eps, bc1, bc2, minLS, maxLS, maxLogit, reg, shLr;
+};
+
+struct ChainArgs {
+  uint32_t n;
+  int V;
+  const DevCam* cams;
+  float* params;
+  float* sh;
+  int32_t* gradP;
+  const uint2* rect;
+  float anisoReg;
+  int32_t* gradCam;
+  float* gradF;            // optional readout (n * 16)
+  float* shGrad;           // optional readout (n * 3K)
+  int doAdam;
+  const AdamHP* hp;        // device-resident (updated every step)
+  float* m;
+  float* v;
+  float* shM;
+  float* shV;
+};
+
+// refine: one spawned splat of the plan the host draws (trainer.js:713-752)
+struct RefineSpawn {
+  uint32_t pos;    // position in the donor list, or in the sorted big-donor list when split
+  uint32_t split;  // 1: split a big donor, 0: clone a donor
+  double g[3];     // the three gauss() jitters of the position
+};
+
+struct RefineApplyArgs {
+  const RefineSpawn* plan;
+  uint32_t count;          // moved + grown
+  uint32_t moved;          // the first `moved` spawns relocate dead splats
+  uint32_t n;              // splat count before growth
+  const uint32_t* deadList;
+  const uint32_t* donorList;
+  const uint32_t* bigSorted;   // donors by mean log-scale, descending (stable)
+  const uint32_t* splitSeq;    // per splat: sequence number of its split, or ~0
+  float* params;
+  float* m;
+  float* v;
+  float* sh;
+  float* shM;
+  float* shV;
+  int shr;                 // 3K
+};
+
+// launchers
+void launch_project(const ProjectArgs& a, int deg, cudaStream_t s);
+void launch_tile_ranges(const TileRangeArgs& a, cudaStream_t s);
+void launch_splat_counts(const SplatCountArgs& a, cudaStream_t s);
+void launch_keygen(const KeygenArgs& a, cudaStream_t s);
+uint32_t scan_partials_needed(uint64_t N);
+void launch_exclusive_scan(const uint32_t* in, uint64_t N, uint32_t* out, uint32_t* partials, uint32_t* total,
+                           cudaStream_t s);
+int onesweep_grid(int device);
+void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s);
+void launch_raster(const RasterArgs& a, int mode, bool stored, int batchDepth, unsigned grid, cudaStream_t s);
+int raster_blocks_per_sm(int batchDepth, int mode);
+void launch_work_order(const uint2* ranges, uint32_t totalTiles, uint32_t* order, cudaStream_t s);
+void launch_chain_adam(const ChainArgs& a, int deg, cudaStream_t s);
+void launch_refine_classify(const float* params, uint32_t n, uint32_t* deadFlag, uint32_t* donorFlag,
+                            cudaStream_t s);
+void launch_refine_compact(const float* params, uint32_t n, const uint32_t* deadFlag, const uint32_t* deadOff,
+                           const uint32_t* donorFlag, const uint32_t* donorOff, uint32_t* deadList,
+                           uint32_t* donorList, uint64_t* donorKeys, uint32_t* donorVals, cudaStream_t s);
+void launch_refine_apply(const RefineApplyArgs& a, uint32_t* splitSeq, cudaStream_t s);
+void launch_max_u32(const uint32_t* x, uint32_t count, uint32_t* out, cudaStream_t s);
+
+}  // namespace gs

@@ -1,0 +1,392 @@
+// gs_sort.cu -- global sorted binning: exclusive scan of per-splat entry
+// counts, and a onesweep LSD radix sort (8-bit digits, decoupled look-back)
+// of the (globalTile << 32 | depth bits, splat id) entries.
+//
+// The reference bins with atomic per-tile cursors and sorts each tile segment
+// with a bitonic network (shaders.js:378-500); its final order is, per tile,
+// ascending (depth f32 bits, id).  Here every entry is keyed by
+// (tile, depth) and written in splat order, so one stable sort over all
+// entries leaves each tile's ids in exactly that order.
+//
+// Onesweep: one histogram kernel reads every key once and counts all digit
+// positions; each digit pass then ranks a 4096-entry block in shared memory
+// (warp ballots give each key its rank among equal digits), publishes the
+// block's per-digit counts, and obtains the count of every earlier block by
+// decoupled look-back before scattering.  Blocks are claimed in order through
+// an atomic counter by a grid that is entirely resident, so every block it
+// waits on is already running.  Each spin has an iteration limit; on expiry
+// the kernel sets ST_LOOKBACK_TIMEOUT in the status word and carries on.
+//
+// Look-back status words are 64-bit: [63:32] epoch tag, [31:30] flag,
+// [29:0] count.  The tag changes every pass of every sort (the histogram
+// kernel advances a device epoch), so words left by earlier sorts read as
+// "not published" and the status array never needs clearing.
+#include <cuda/atomic>
+
+#include "gs_common.cuh"
+#include "gs_kernels.h"
+
+namespace gs {
+
+// ---------------------------------------------------------------------------
+// Exclusive scan of u32 counts (3 phases: block sums, scan of block sums,
+// block rescans).  Block = 1024 threads x 4 items.
+// ---------------------------------------------------------------------------
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_BLOCK = 1024 * SCAN_ITEMS;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan_1024(uint32_t x, uint32_t* s_warp, uint32_t* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) s_warp[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t w = s_warp[lane];
+    uint32_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    s_warp[lane] = wi - w;
+    if (lane == 31) s_warp[32] = wi;
+  }
+  __syncthreads();
+  const uint32_t r = s_warp[wid] + inc - x;
+  if (total) *total = s_warp[32];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_reduce(const uint32_t* in, uint64_t N, uint32_t* partials) {
+  __shared__ uint32_t s_warp[33];
+  const uint64_t base = (uint64_t)blockIdx.x * SCAN_BLOCK + (uint64_t)threadIdx.x * SCAN_ITEMS;
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k)
+    if (base + k < N) s += in[base + k];
+  uint32_t tot;
+  block_exclusive_scan_1024(s, s_warp, &tot);
+  if (threadIdx.x == 0) partials[blockIdx.x] = tot;
+}
+
+// single block: exclusive scan of the block sums, total to *total
+__global__ void __launch_bounds__(1024) k_scan_partials(uint32_t* partials, uint32_t nb, uint32_t* total) {
+  __shared__ uint32_t s_warp[33];
+  __shared__ uint32_t s_carry;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (uint32_t base = 0; base < nb; base += 1024 * SCAN_ITEMS) {
+    const uint32_t i0 = base + threadIdx.x * SCAN_ITEMS;
+    uint32_t v[SCAN_ITEMS];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) { v[k] = (i0 + k < nb) ? partials[i0 + k] : 0u; s += v[k]; }
+    uint32_t tot;
+    uint32_t ex = block_exclusive_scan_1024(s, s_warp, &tot) + s_carry;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+      if (i0 + k < nb) partials[i0 + k] = ex;
+      ex += v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = s_carry;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_down(const uint32_t* in, uint64_t N, const uint32_t* partials,
+                                                    uint32_t* out) {
+  __shared__ uint32_t s_warp[33];
+  const uint64_t base = (uint64_t)blockIdx.x * SCAN_BLOCK + (uint64_t)threadIdx.x * SCAN_ITEMS;
+  uint32_t v[SCAN_ITEMS];
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) { v[k] = (base + k < N) ? in[base + k] : 0u; s += v[k]; }
+  uint32_t ex = block_exclusive_scan_1024(s, s_warp, nullptr) + partials[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    if (base + k < N) out[base + k] = ex;
+    ex += v[k];
+  }
+}
+
+uint32_t scan_partials_needed(uint64_t N) { return (uint32_t)((N + SCAN_BLOCK - 1) / SCAN_BLOCK); }
+
+void launch_exclusive_scan(const uint32_t* in, uint64_t N, uint32_t* out, uint32_t* partials, uint32_t* total,
+                           cudaStream_t s) {
+  const uint32_t nb = scan_partials_needed(N);
+  if (nb == 0) { cudaMemsetAsync(total, 0, 4, s); return; }
+  k_scan_reduce<<<nb, 1024, 0, s>>>(in, N, partials);
+  k_scan_partials<<<1, 1024, 0, s>>>(partials, nb, total);
+  k_scan_down<<<nb, 1024, 0, s>>>(in, N, partials, out);
+}
+
+// ---------------------------------------------------------------------------
+// Onesweep radix sort.
+// ---------------------------------------------------------------------------
+constexpr int RS_THREADS = 256;
+constexpr int RS_WARPS = RS_THREADS / 32;
+constexpr int RS_ITEMS = 16;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;  // 4096 entries per block
+constexpr int RS_MAX_PASSES = 8;
+constexpr uint32_t FLAG_AGG = 1u, FLAG_INC = 2u;
+constexpr uint32_t LOOKBACK_SPIN_LIMIT = 1u << 22;
+
+// Histogram of every digit position: one read of all keys.
+__global__ void __launch_bounds__(256) k_radix_hist(RadixHistArgs a) {
+  __shared__ uint32_t h[RS_MAX_PASSES][256];
+  for (int i = threadIdx.x; i < RS_MAX_PASSES * 256; i += blockDim.x) (&h[0][0])[i] = 0;
+  __syncthreads();
+  const uint32_t N = *a.nItems;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const uint64_t k = a.keys[i];
+    for (int p = 0; p < a.passes; ++p) atomicAdd(&h[p][(k >> (8 * p)) & 0xFF], 1u);
+  }
+  __syncthreads();
+  for (int p = 0; p < a.passes; ++p)
+    for (int d = threadIdx.x; d < 256; d += blockDim.x)
+      if (h[p][d]) atomicAdd(&a.hist[p * 256 + d], h[p][d]);
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.epoch[0] = a.epoch[0] + 1u;
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__global__ void __launch_bounds__(RS_THREADS) k_onesweep(OnesweepArgs a) {
+  extern __shared__ __align__(16) unsigned char rs_dyn[];
+  uint64_t* s_keys = reinterpret_cast<uint64_t*>(rs_dyn);                  // RS_TILE keys
+  uint32_t* s_vals = reinterpret_cast<uint32_t*>(rs_dyn + RS_TILE * 8);     // RS_TILE values
+  __shared__ uint32_t s_whist[RS_WARPS][256];
+  __shared__ uint32_t s_count[256];     // this block's count per digit
+  __shared__ uint32_t s_local[256];     // exclusive prefix of s_count over digits
+  __shared__ uint32_t s_gbase[256];     // global start of this block's run per digit
+  __shared__ uint32_t s_dbase[256];     // exclusive scan of the pass histogram
+  __shared__ uint32_t s_warp[33];
+  __shared__ uint32_t s_tile;
+
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const uint32_t N = *a.nItems;
+  const uint32_t numTiles = (N + RS_TILE - 1) / RS_TILE;
+  const uint32_t tag = a.epoch[0] * RS_MAX_PASSES + (uint32_t)a.pass + 1u;
+  const int shift = 8 * a.pass;
+
+  // global digit bases: exclusive scan of this pass's histogram (256 threads)
+  {
+    const uint32_t hv = a.hist[a.pass * 256 + tid];
+    uint32_t inc = hv;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    if (lane == 31) s_warp[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+      uint32_t w = lane < RS_WARPS ? s_warp[lane] : 0u, wi = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+        if (lane >= o) wi += y;
+      }
+      if (lane < RS_WARPS) s_warp[lane] = wi - w;
+    }
+    __syncthreads();
+    s_dbase[tid] = s_warp[wid] + inc - hv;
+    __syncthreads();
+  }
+
+  for (;;) {
+    if (tid == 0) s_tile = atomicAdd(a.tileCounter + a.pass, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    if (tile >= numTiles) break;
+    const uint32_t base = tile * RS_TILE;
+
+    // load: warp w holds entries [base + w*512, +512), item j at lane l
+    uint64_t key[RS_ITEMS];
+    uint32_t val[RS_ITEMS];
+    uint32_t dig[RS_ITEMS];
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; ++j) {
+      const uint32_t idx = base + wid * (32 * RS_ITEMS) + j * 32 + lane;
+      if (idx < N) {
+        key[j] = a.keysIn[idx];
+        val[j] = a.valsIn[idx];
+        dig[j] = (uint32_t)(key[j] >> shift) & 0xFFu;
+      } else {
+        key[j] = 0; val[j] = 0; dig[j] = 0x100u;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 256 / 32; ++k) s_whist[wid][lane + 32 * k] = 0;
+    __syncwarp();
+
+    // rank within the warp, items in order, lanes in order
+    uint32_t rank[RS_ITEMS];
+    const uint32_t ltm = lanemask_lt();
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; ++j) {
+      const bool valid = dig[j] < 0x100u;
+      uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, (dig[j] >> b) & 1u);
+        peers &= ((dig[j] >> b) & 1u) ? bal : ~bal;
+      }
+      uint32_t pre = 0;
+      if (valid) pre = s_whist[wid][dig[j]];
+      __syncwarp();
+      if (valid) {
+        const uint32_t below = __popc(peers & ltm);
+        rank[j] = pre + below;
+        if (below == 0) s_whist[wid][dig[j]] = pre + __popc(peers);
+      } else {
+        rank[j] = 0;
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+
+    // per digit: exclusive scan across warps, block count
+    {
+      const int d = tid;
+      uint32_t run = 0;
+#pragma unroll
+      for (int w = 0; w < RS_WARPS; ++w) {
+        const uint32_t c = s_whist[w][d];
+        s_whist[w][d] = run;
+        run += c;
+      }
+      s_count[d] = run;
+
+      // decoupled look-back for digit d
+      cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> my(
+          *reinterpret_cast<unsigned long long*>(a.status + (size_t)tile * 256 + d));
+      uint32_t excl = 0;
+      if (tile == 0) {
+        my.store(((unsigned long long)tag << 32) | ((unsigned long long)FLAG_INC << 30) | run,
+                 cuda::memory_order_relaxed);
+      } else {
+        my.store(((unsigned long long)tag << 32) | ((unsigned long long)FLAG_AGG << 30) | run,
+                 cuda::memory_order_relaxed);
+        int64_t t = (int64_t)tile - 1;
+        uint32_t spins = 0;
+        while (t >= 0) {
+          cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> pr(
+              *reinterpret_cast<unsigned long long*>(a.status + (size_t)t * 256 + d));
+          const unsigned long long s = pr.load(cuda::memory_order_relaxed);
+          const uint32_t stag = (uint32_t)(s >> 32);
+          const uint32_t flag = (uint32_t)(s >> 30) & 3u;
+          if (stag != tag || flag == 0) {
+            if (++spins > LOOKBACK_SPIN_LIMIT) { atomicOr(a.statusWord, ST_LOOKBACK_TIMEOUT); break; }
+            __nanosleep(32);
+            continue;
+          }
+          excl += (uint32_t)(s & 0x3FFFFFFFull);
+          if (flag == FLAG_INC) break;
+          --t;
+        }
+        my.store(((unsigned long long)tag << 32) | ((unsigned long long)FLAG_INC << 30) | (excl + run),
+                 cuda::memory_order_relaxed);
+      }
+      s_gbase[d] = s_dbase[d] + excl;
+    }
+    // exclusive scan of s_count over digits -> s_local
+    {
+      const uint32_t cv = s_count[tid];
+      uint32_t inc = cv;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+        if (lane >= o) inc += y;
+      }
+      __syncthreads();
+      if (lane == 31) s_warp[wid] = inc;
+      __syncthreads();
+      if (wid == 0) {
+        uint32_t w = lane < RS_WARPS ? s_warp[lane] : 0u, wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+          if (lane >= o) wi += y;
+        }
+        if (lane < RS_WARPS) s_warp[lane] = wi - w;
+      }
+      __syncthreads();
+      s_local[tid] = s_warp[wid] + inc - cv;
+    }
+    __syncthreads();
+
+    // stage in shared memory in sorted order
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; ++j) {
+      if (dig[j] < 0x100u) {
+        const uint32_t pos = s_local[dig[j]] + s_whist[wid][dig[j]] + rank[j];
+        s_keys[pos] = key[j];
+        s_vals[pos] = val[j];
+      }
+    }
+    __syncthreads();
+    const uint32_t cnt = min((uint32_t)RS_TILE, N - base);
+    for (uint32_t i = tid; i < cnt; i += RS_THREADS) {
+      const uint64_t k = s_keys[i];
+      const uint32_t d = (uint32_t)(k >> shift) & 0xFFu;
+      const uint32_t g = s_gbase[d] + (i - s_local[d]);
+      if (a.keysOut) a.keysOut[g] = k;
+      a.valsOut[g] = s_vals[i];
+    }
+    __syncthreads();
+  }
+}
+
+constexpr size_t RS_DYN_SMEM = (size_t)RS_TILE * 12;
+
+int onesweep_grid(int device) {
+  int sms = 0, perSm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS_DYN_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_onesweep, RS_THREADS, RS_DYN_SMEM);
+  if (perSm < 1) perSm = 1;
+  return sms * perSm;
+}
+
+// Sorts N = *nItems entries (N known only on the device) on key bits
+// [0, 8*passes).  Result lands in (keys,vals)[passes & 1 ? 1 : 0] of the
+// ping-pong pair.  hist must hold passes*256 u32, tileCounter passes u32;
+// the caller clears both before the call.
+void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s) {
+  RadixHistArgs h;
+  h.keys = a.keys[0];
+  h.nItems = a.nItems;
+  h.hist = a.hist;
+  h.passes = a.passes;
+  h.epoch = a.epoch;
+  k_radix_hist<<<a.histGrid, 256, 0, s>>>(h);
+  for (int p = 0; p < a.passes; ++p) {
+    OnesweepArgs o;
+    o.keysIn = a.keys[p & 1];
+    o.valsIn = a.vals[p & 1];
+    o.keysOut = (p == a.passes - 1 && !a.keepKeys) ? nullptr : a.keys[(p + 1) & 1];
+    o.valsOut = a.vals[(p + 1) & 1];
+    o.nItems = a.nItems;
+    o.hist = a.hist;
+    o.tileCounter = a.tileCounter;
+    o.status = a.status;
+    o.statusWord = a.statusWord;
+    o.epoch = a.epoch;
+    o.pass = p;
+    k_onesweep<<<a.sweepGrid, RS_THREADS, RS_DYN_SMEM, s>>>(o);
+  }
+}
+
+}  // namespace gs

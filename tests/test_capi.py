@@ -1,0 +1,63 @@
+"""The C ABI without a GPU: the library builds, loads, and exports every
+entry point include/splat_b200.h declares; defaults mirror the reference's
+GSTrainer options (src/gs/trainer.js:18-49)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from splat_b200 import native as N
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "splat_b200.h")).read()
+    return sorted(set(re.findall(r"GS_API\s+[\w\s\*]*?\b(gs_\w+)\s*\(", src)))
+
+
+def test_library_builds_and_exports_every_declared_symbol():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("gs_build", os.path.join(ROOT, "splat.js_b200", "build.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    path = mod.build()
+    assert os.path.exists(path)
+    syms = declared_symbols()
+    assert len(syms) >= 25, syms
+    L = C.CDLL(path)
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+    # the binding covers the header exactly
+    N.lib()
+    assert N.lib().gs_abi_version() == 1
+
+
+def test_default_options_match_reference():
+    o = N.GsOptions()
+    assert N.lib().gs_default_options(C.byref(o)) == 0
+    assert o.eCut == pytest.approx(4.5) and o.aMin == pytest.approx(0.0039)
+    assert o.radClamp == 1.0 and o.anisoReg == pytest.approx(0.005)
+    assert o.shDeg == 2 and o.tileGrad == 1 and o.capMult == 4.0 and o.maxIters == 60000
+    assert o.minScale == pytest.approx(1e-4) and o.opacityReg == pytest.approx(0.01)
+    assert o.shLr == pytest.approx(1.25e-4) and o.growRate == pytest.approx(0.15)
+    assert o.tile == 16
+
+
+def test_struct_sizes_match_header():
+    # gs_options: 4 f32, 2 i32, u64, u32, f32, u32, 5 f32, 7 i32 -> 80 bytes with padding
+    assert C.sizeof(N.GsCamera) == 4 * (9 + 3 + 3 + 2 + 1 + 2)
+    assert C.sizeof(N.GsImage) == 16
+    assert C.sizeof(N.GsRefineResult) == 24
+
+
+def test_create_without_device_fails_cleanly():
+    """On a host with no GPU gs_create reports an error instead of falling back."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    h = C.c_void_p()
+    rc = N.lib().gs_create(None, C.byref(h))
+    assert rc != 0
+    assert b"device" in N.lib().gs_last_error(None)

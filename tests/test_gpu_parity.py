@@ -1,0 +1,351 @@
+"""CUDA path against the CPU oracle, through the C ABI (B200 required).
+
+Both sides perform the same FP32 operations in the same order (canonical
+exp/log, explicit fused multiply-adds, IEEE division, i32 fixed-point
+gradient sums), so every comparison below is bit-exact: projection records,
+per-tile ordered id lists, images, final transmittance, end indices,
+fixed-point screen-space gradients, parameter gradients, updated parameters
+and Adam moments.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+import rigs
+from splat_b200 import scene
+from splat_b200.trainer import GSTrainer
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_cam(meta, ci, ncams, activeSh, train=1):
+    return O.cam(meta["R"], meta["t"], meta["f"], meta["cx"], meta["cy"], meta["w"], meta["h"],
+                 gain=float(np.float32(math.exp(meta.get("g", 0.0) or 0.0))), bias=meta.get("b", 0.0) or 0.0,
+                 offset=meta["offset"], camIdx=ci, ncams=ncams, activeSh=float(activeSh), train=train)
+
+
+def make(params, sh, cams, rgbs, opts, radius=1.5, maxW=None, maxH=None):
+    images = [dict(tw=c["w"], th=c["h"], rgb=rgbs[k]) for k, c in enumerate(cams)]
+    for k, c in enumerate(cams):
+        c["imgIdx"] = k
+    t = GSTrainer.create(dict(opts))
+    n = len(params) // 16
+    t.setup(dict(data=params, n=n, sh=sh), cams, images, maxW or max(c["w"] for c in cams),
+            maxH or max(c["h"] for c in cams), radius)
+    targets, metas = scene.pack_targets(images, cams)
+    return t, targets, metas
+
+
+def oracle_opts(opts):
+    return O.opts(eCut=opts.get("eCut", 4.5), aMin=opts.get("aMin", 0.0039), radClamp=opts.get("radClamp", 1.0),
+                  anisoReg=opts.get("anisoReg", 0.005), shDeg=opts.get("shDeg", 2),
+                  entriesCap=opts.get("entriesCap", 12_000_000))
+
+
+def gpu_raster(t, cis, mode=3):
+    import ctypes as C
+    from splat_b200 import native as N
+    arr = (C.c_uint32 * len(cis))(*cis)
+    N.check(N.lib().gs_raster_pass(t._h, arr, len(cis), mode), t._h)
+
+
+def gpu_view(t, view, meta, n):
+    import ctypes as C
+    from splat_b200 import native as N
+    L = N.lib()
+    rec = np.zeros(n * 12, np.float32)
+    rect = np.zeros(n * 2, np.uint32)
+    N.check(L.gs_debug_records(t._h, view, N.ptr(rec), N.ptr(rect, C.c_uint32)), t._h)
+    nt = ((meta["w"] + 15) // 16) * ((meta["h"] + 15) // 16)
+    cnt = np.zeros(nt, np.uint32)
+    rg = np.zeros(nt * 2, np.uint32)
+    nE = C.c_uint64()
+    N.check(L.gs_debug_binning(t._h, view, N.ptr(cnt, C.c_uint32), N.ptr(rg, C.c_uint32), None, 0, C.byref(nE)),
+            t._h)
+    ids = np.zeros(max(1, nE.value), np.uint32)
+    N.check(L.gs_debug_binning(t._h, view, None, None, N.ptr(ids, C.c_uint32), nE.value, C.byref(nE)), t._h)
+    np_ = meta["w"] * meta["h"]
+    img = np.zeros(np_ * 4, np.float32)
+    fT = np.zeros(np_, np.float32)
+    end = np.zeros(np_, np.uint32)
+    N.check(L.gs_debug_pixels(t._h, view, N.ptr(img), N.ptr(fT), N.ptr(end, C.c_uint32)), t._h)
+    gp = np.zeros(n * 10, np.int32)
+    N.check(L.gs_debug_gradp(t._h, view, N.ptr(gp, C.c_int32), 1), t._h)
+    return dict(rec=rec, rect=rect, cnt=cnt, ranges=rg.reshape(-1, 2), ids=ids[:nE.value], img=img, finalT=fT,
+                end=end, gradP=gp.reshape(-1, 10))
+
+
+def assert_bits(a, b, what):
+    a = np.ascontiguousarray(a)
+    b = np.ascontiguousarray(b)
+    assert a.shape == b.shape, (what, a.shape, b.shape)
+    if a.dtype.kind == "f":
+        same = a.view(np.uint32 if a.dtype == np.float32 else np.uint64) == b.view(
+            np.uint32 if b.dtype == np.float32 else np.uint64)
+        # +0 / -0 and NaN payloads are not expected; compare bit patterns
+    else:
+        same = a == b
+    bad = np.flatnonzero(~same.reshape(-1))
+    assert bad.size == 0, f"{what}: {bad.size} of {same.size} differ, first at {bad[:5]}: " \
+                          f"{a.reshape(-1)[bad[:5]]} vs {b.reshape(-1)[bad[:5]]}"
+
+
+def check_view_against_oracle(t, o, ocam, params, sh, targets, n, view=0):
+    g = gpu_view(t, view, dict(w=ocam.w, h=ocam.h), n)
+    proj = O.project(o, ocam, params, sh if o.shDeg else None, n)
+    rec, rect = O.records(o, ocam, proj, n)
+    vis = rect[0::2] != 0xFFFFFFFF
+    assert_bits(g["rect"], rect, "tile rects")
+    assert_bits(g["rec"].reshape(-1, 12)[vis], rec.reshape(-1, 12)[vis], "projection records")
+    b = O.bin_tiles(o, ocam, proj, n)
+    assert_bits(g["cnt"], b["cnt"], "per-tile counts (tileCnt)")
+    base = g["ranges"][0, 0]
+    assert_bits(g["ranges"][:, 0] - base, b["start"][:-1], "tile starts")
+    assert_bits(g["ranges"][:, 1] - base, b["start"][1:], "tile ends")
+    assert_bits(g["ids"][base:base + len(b["ids"])], b["ids"], "per-tile ordered ids (sort permutation)")
+    r = O.render(o, ocam, proj, b, targets, n, train=True, ncams=ocam.ncams)
+    assert_bits(g["img"], r["img"], "image")
+    assert_bits(g["finalT"], r["finalT"], "final transmittance")
+    assert_bits(g["end"], r["end"], "end indices")
+    assert_bits(g["gradP"], r["gradP"].reshape(-1, 16)[:, :10], "fixed-point screen-space gradients")
+    return g, r, proj, b
+
+
+def rig_setup(sh_deg=3):
+    n = 160
+    params = rigs.gradcheck_params(n)
+    K = O.sh_rest(sh_deg)
+    sh, _ = rigs.gradcheck_sh(n, K)
+    rgb = rigs.gradcheck_rgb()
+    cams = [dict(R=[1, 0, 0, 0, 1, 0, 0, 0, 1], t=[0, 0, 0], f=60.0, cx=32.0, cy=32.0, w=64, h=64)]
+    opts = dict(shDeg=sh_deg, **rigs.STRICT)
+    return params, sh, cams, [rgb], opts, n
+
+
+def test_gradcheck_rig_raster_bitexact():
+    params, sh, cams, rgbs, opts, n = rig_setup()
+    t, targets, metas = make(params, sh, cams, rgbs, opts)
+    gpu_raster(t, [0], 3)
+    o = oracle_opts(opts)
+    c = oracle_cam(metas[0], 0, 1, opts["shDeg"])
+    check_view_against_oracle(t, o, c, params, sh, targets, n)
+
+
+def test_gradcheck_rig_grad_pass_bitexact():
+    params, sh, cams, rgbs, opts, n = rig_setup()
+    t, targets, metas = make(params, sh, cams, rgbs, opts)
+    gF, sG, st = t.gradPass(0)
+    o = oracle_opts(opts)
+    c = oracle_cam(metas[0], 0, 1, opts["shDeg"])
+    K = O.sh_rest(opts["shDeg"])
+    z = np.zeros(n * 16, np.float32)
+    zs = np.zeros(n * 3 * K, np.float32)
+    stats = np.zeros(4, np.uint32)
+    r = O.step(o, [c], O.adam_hp([0] * 16, 1, -10, 0), params.copy(), sh.copy(), targets, z.copy(), z.copy(),
+               zs.copy(), zs.copy(), n, stats=stats, do_adam=False)
+    assert_bits(gF, r["gradF"], "gradF")
+    assert_bits(sG, r["shGrad"], "shGrad")
+    assert_bits(st, stats, "stats")
+
+
+def config0(n=20000, seed=0):
+    params, sh = scene.uniform_scene(n, seed=seed, sh_deg=2)
+    R, tt = scene.look_at_pose([0.0, 0.0, -3.0], [0.0, 0.0, 0.0])
+    cams = [dict(R=R, t=tt, f=300.0, cx=128.0, cy=128.0, w=256, h=256)]
+    rgbs = [scene.uniform_target(256, 256, seed=seed)]
+    return params, sh, cams, rgbs
+
+
+def oracle_adam(t, iter_after, radius, horizon=60000, opacityReg=0.01, shLr=1.25e-4):
+    base = 3e-4 * radius
+    pos = base * math.pow(0.01, min(1.0, iter_after / (0.75 * horizon)))
+    lr = [pos, pos, pos, 5e-3, 5e-3, 5e-3, 1e-3, 1e-3, 1e-3, 1e-3, 1.5e-2, 1.5e-2, 1.5e-2, 2.5e-2, 0, 0]
+    lr = [float(np.float32(x)) for x in lr]
+    return O.adam_hp(lr, iter_after, float(np.float32(math.log(radius * 1e-4))),
+                     float(np.float32(math.log(radius * 0.05))), reg=opacityReg, shLr=shLr)
+
+
+def test_config0_raster_bitexact():
+    params, sh, cams, rgbs = config0()
+    n = len(params) // 16
+    t, targets, metas = make(params, sh, cams, rgbs, dict(shDeg=2), radius=1.0)
+    gpu_raster(t, [0], 3)
+    check_view_against_oracle(t, oracle_opts(dict(shDeg=2)), oracle_cam(metas[0], 0, 1, 2), params, sh, targets, n)
+
+
+@pytest.mark.parametrize("steps", [3])
+def test_config0_training_steps_bitexact(steps):
+    """Full steps (project, sort, raster, chain, Adam, SH-Adam) at iter 2000+
+    (all SH bands active): parameters, SH and Adam moments after each step."""
+    params, sh, cams, rgbs = config0()
+    n = len(params) // 16
+    K = 8
+    t, targets, metas = make(params, sh, cams, rgbs, dict(shDeg=2), radius=1.0)
+    t.iter = 2000
+    o = oracle_opts(dict(shDeg=2))
+    p, s = params.copy(), sh.copy()
+    m = np.zeros(n * 16, np.float32)
+    v = np.zeros(n * 16, np.float32)
+    sm = np.zeros(n * 3 * K, np.float32)
+    sv = np.zeros(n * 3 * K, np.float32)
+    stats = np.zeros(4, np.uint32)
+    for k in range(steps):
+        t.stepBatch([0])
+        it = 2000 + k + 1
+        c = oracle_cam(metas[0], 0, 1, 2)
+        O.step(o, [c], oracle_adam(t, it, 1.0), p, s, targets, m, v, sm, sv, n, stats=stats)
+        g = t.readGaussians()
+        assert_bits(g["data"], p, f"params after step {k + 1}")
+        assert_bits(g["sh"], s, f"SH after step {k + 1}")
+    gm, gv, gsm, gsv = t.readMoments()
+    assert_bits(gm, m, "Adam m")
+    assert_bits(gv, v, "Adam v")
+    assert_bits(gsm, sm, "SH-Adam m")
+    assert_bits(gsv, sv, "SH-Adam v")
+    st = np.zeros(4, np.uint32)
+    import ctypes as C
+    from splat_b200 import native as N
+    N.check(N.lib().gs_read_stats(t._h, N.ptr(st, C.c_uint32)), t._h)
+    assert_bits(st, stats, "accumulated stats")
+
+
+def test_batched_uneven_views_bitexact():
+    """One optimiser step over three views of different resolutions: the
+    per-view rasters match the oracle and the summed gradients and update
+    equal the oracle's batched step."""
+    n = 6000
+    params, sh = scene.surface_scene(n, seed=3, sh_deg=2, log_scale=(-3.5, 0.5))
+    res = [(160, 96), (96, 64), (200, 120)]
+    cams = []
+    for k, (w, h) in enumerate(res):
+        cc = scene.ring_cameras(3, 4.0, 0.5, w, h, phase=0.3)[k]
+        cams.append(cc)
+    rgbs = [scene.uniform_target(w, h, seed=10 + k) for k, (w, h) in enumerate(res)]
+    t, targets, metas = make(params, sh, cams, rgbs, dict(shDeg=2, maxBatch=4), radius=2.0)
+    t.iter = 2000
+    o = oracle_opts(dict(shDeg=2))
+    gpu_raster(t, [0, 1, 2], 3)
+    for v in range(3):
+        check_view_against_oracle(t, o, oracle_cam(metas[v], v, 3, 2), params, sh, targets, n, view=v)
+    K = 8
+    m = np.zeros(n * 16, np.float32)
+    vv = np.zeros(n * 16, np.float32)
+    sm = np.zeros(n * 3 * K, np.float32)
+    sv = np.zeros(n * 3 * K, np.float32)
+    p, s = params.copy(), sh.copy()
+    t.stepBatch([0, 1, 2])
+    ocams = [oracle_cam(metas[v], v, 3, 2) for v in range(3)]
+    O.step(o, ocams, oracle_adam(t, 2001, 2.0), p, s, targets, m, vv, sm, sv, n)
+    g = t.readGaussians()
+    assert_bits(g["data"], p, "params after a batched step")
+    assert_bits(g["sh"], s, "SH after a batched step")
+
+
+def test_stored_state_variant_matches_recompute():
+    """The stored-state backward reads the forward's T instead of dividing:
+    images are bit-identical, gradients agree within 1e-4 (relative, norm)."""
+    params, sh, cams, rgbs = config0(n=8000, seed=5)
+    n = len(params) // 16
+    t0, targets, metas = make(params, sh, cams, rgbs, dict(shDeg=2), radius=1.0)
+    t1, _, _ = make(params, sh, cams, rgbs, dict(shDeg=2, backwardVariant=1), radius=1.0)
+    g0, s0, st0 = t0.gradPass(0)
+    g1, s1, st1 = t1.gradPass(0)
+    assert_bits(st0, st1, "stats (forward and loss are shared)")
+    rel = np.linalg.norm(g1 - g0) / np.linalg.norm(g0)
+    assert rel < 1e-4, rel
+    o = oracle_opts(dict(shDeg=2))
+    c = oracle_cam(metas[0], 0, 1, 2)
+    z = np.zeros(n * 16, np.float32)
+    zs = np.zeros(n * 24, np.float32)
+    r = O.step(o, [c], O.adam_hp([0] * 16, 1, -10, 0), params.copy(), sh.copy(), targets, z.copy(), z.copy(),
+               zs.copy(), zs.copy(), n, do_adam=False, variant=1)
+    assert_bits(g1, r["gradF"], "stored-state gradF vs oracle stored-state")
+
+
+def test_runs_are_bitwise_deterministic():
+    params, sh, cams, rgbs = config0(n=10000, seed=2)
+    out = []
+    for _ in range(2):
+        t, targets, metas = make(params, sh, cams, rgbs, dict(shDeg=2), radius=1.0)
+        t.iter = 2000
+        for _ in range(2):
+            t.stepBatch([0])
+        out.append(t.readGaussians()["data"])
+    assert_bits(out[0], out[1], "two identical runs")
+
+
+def test_entry_budget_drops_match_reference_rule():
+    """A small entry budget drops whole tiles exactly as the reference's scan
+    (shaders.js:357-372) does, and counts them in stats[3]."""
+    params, sh, cams, rgbs = config0(n=20000, seed=0)
+    n = len(params) // 16
+    opts = dict(shDeg=2, entriesCap=20000)
+    t, targets, metas = make(params, sh, cams, rgbs, opts, radius=1.0)
+    gpu_raster(t, [0], 3)
+    o = oracle_opts(opts)
+    c = oracle_cam(metas[0], 0, 1, 2)
+    proj = O.project(o, c, params, sh, n)
+    b = O.bin_tiles(o, c, proj, n)
+    assert b["overflow"] > 0
+    g = gpu_view(t, 0, metas[0], n)
+    assert_bits(g["ranges"][:, 1] - g["ranges"][:, 0], np.diff(b["start"]), "kept counts per tile")
+    base = g["ranges"][0, 0]
+    assert_bits(g["ids"][base:base + len(b["ids"])], b["ids"], "kept ids")
+    st = t.readLoss()
+    assert t.entryOverflowTiles == b["overflow"]
+
+
+def test_render_view_matches_oracle_forward():
+    params, sh, cams, rgbs = config0(n=20000, seed=1)
+    n = len(params) // 16
+    t, targets, metas = make(params, sh, cams, rgbs, dict(shDeg=2), radius=1.0)
+    view = dict(metas[0])
+    img = t.renderView(view)
+    o = oracle_opts(dict(shDeg=2))
+    c = oracle_cam(view, 0, 1, 2, train=0)
+    proj = O.project(o, c, params, sh, n)
+    b = O.bin_tiles(o, c, proj, n)
+    r = O.render(o, c, proj, b, targets, n, train=False)
+    assert_bits(img.reshape(-1), r["img"], "renderView image")
+
+
+def test_refine_matches_oracle():
+    """Device refine vs the restated JavaScript refine with the same rng draws."""
+    n = 4000
+    params, sh = scene.uniform_scene(n, seed=7, sh_deg=2)
+    P = params.reshape(-1, 16)
+    rng0 = np.random.default_rng(9)
+    P[:, 13] = rng0.normal(-1.0, 3.0, n)   # many dead and many donors
+    params = P.reshape(-1)
+    R, tt = scene.look_at_pose([0.0, 0.0, -3.0], [0.0, 0.0, 0.0])
+    cams = [dict(R=R, t=tt, f=150.0, cx=64.0, cy=64.0, w=128, h=128)]
+    rgbs = [scene.uniform_target(128, 128)]
+    t, targets, metas = make(params, sh, cams, rgbs, dict(shDeg=2, maxSplats=8000), radius=1.0)
+    t.iter = 2000
+    t.stepBatch([0])
+    g = t.readGaussians()
+    m, v, sm, sv = t.readMoments()
+    cap = t.cap
+    K = 8
+    op = np.zeros(cap * 16, np.float32); op[:n * 16] = g["data"]
+    om = np.zeros(cap * 16, np.float32); om[:n * 16] = m
+    ov = np.zeros(cap * 16, np.float32); ov[:n * 16] = v
+    osh = np.zeros(cap * 3 * K, np.float32); osh[:n * 3 * K] = g["sh"]
+    osm = np.zeros(cap * 3 * K, np.float32); osm[:n * 3 * K] = sm
+    osv = np.zeros(cap * 3 * K, np.float32); osv[:n * 3 * K] = sv
+    r_cpu = O.refine(n, cap, op, om, ov, osh, osm, osv, K, rigs.lcg(31337), t.iter, 0.75 * 60000)
+    r_gpu = t.refine(rigs.lcg(31337))
+    assert r_gpu["moved"] == r_cpu["moved"] and r_gpu["grown"] == r_cpu["grown"] and r_gpu["n"] == r_cpu["n"]
+    n2 = r_gpu["n"]
+    g2 = t.readGaussians()
+    m2, v2, sm2, sv2 = t.readMoments()
+    assert_bits(g2["data"], op[:n2 * 16], "params after refine")
+    assert_bits(g2["sh"], osh[:n2 * 3 * K], "SH after refine")
+    assert_bits(m2, om[:n2 * 16], "m after refine")
+    assert_bits(v2, ov[:n2 * 16], "v after refine")
+    assert_bits(sm2, osm[:n2 * 3 * K], "SH m after refine")
+    # and training continues on the grown model
+    t.stepBatch([0])
+    assert t.readGaussians()["n"] == n2
