@@ -1,0 +1,432 @@
+"""Training-step benchmark: train views/s at 1M splats, 1920x1080, SH degree 2.
+
+Workload (the metric's configuration): a seeded 1,000,000-splat surface
+scene (60% on three planes, 30% on a unit sphere, 10% on a radius-20 shell;
+log-scales N(-5, 0.7)), SH degree 2 with all bands active (iteration counter
+started at 2000), 24 ring cameras at 1920x1080 (f = 1.171875 W), targets
+rendered from a perturbed copy of the scene (N(0, 0.02) on every
+parameter).  A step is one optimiser step: the batched step renders and
+backpropagates 8 views in one graph-captured launch sequence; the plain
+step is the reference's stepOnce (one view).  `value` is the batched
+step's views/s (device-resident inputs); the plain step's views/s is
+reported beside it.  The working set (params, Adam moments, SH, entries)
+is several GB, larger than the 126 MB L2, so no flush is needed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the CPU restatement of the reference's step (the
+oracle, all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "splat.js_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "train views/s @1M splats 1080p, batched vs plain step, 1 B200, grads within 1e-4"
+FLOP_PER_PAIR = 26 + 70   # raster forward + backward per evaluated pixel-entry pair (FFMA = 2)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--splats", type=int, default=1_000_000)
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--cams", type=int, default=24)
+    ap.add_argument("--batch-depth", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--seed", type=int, default=0)
+    return ap.parse_args()
+
+
+def workload(args):
+    from splat_b200 import scene
+    params, sh = scene.surface_scene(args.splats, seed=args.seed, sh_deg=2, log_scale=(-5.0, 0.7))
+    cams = scene.ring_cameras(args.cams, 4.0, 0.5, args.width, args.height)
+    for k, c in enumerate(cams):
+        c["imgIdx"] = k
+    return params, sh, cams
+
+
+def config_dict(args, extra=None):
+    d = {"workload": f"{args.splats // 1000}k-splat surface scene, SH deg 2, {args.width}x{args.height}, "
+                     f"batch of {args.batch} views per step",
+         "splats": args.splats, "resolution": f"{args.width}x{args.height}", "views_per_batched_step": args.batch,
+         "cameras": args.cams, "sh_degree": 2, "tile": 16, "l2": "working set > L2 (no flush needed)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+        try:
+            import torch
+            self.device = "GPU-" + str(torch.cuda.get_device_properties(device).uuid)
+        except Exception:
+            pass
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                self.out, _ = self.p.communicate()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU side (oracle): baseline sample and the --impl reference arm
+# ---------------------------------------------------------------------------
+def cpu_view_sample(args, params, sh, cams, targets, offsets, ci=0, tile_stride=16):
+    """One plain step of camera ci on the host: project, bin, chain and Adam in
+    full, the raster on every tile_stride-th tile, scaled to a full view."""
+    from oracle import oracle as O
+    n = len(params) // 16
+    K = 8
+    o = O.opts(shDeg=2, entriesCap=max(12_000_000, n * 24))
+    c = cams[ci]
+    oc = O.cam(c["R"], c["t"], c["f"], c["cx"], c["cy"], c["w"], c["h"], offset=offsets[ci], camIdx=ci,
+               ncams=len(cams), activeSh=2.0)
+    t0 = time.perf_counter()
+    proj = O.project(o, oc, params, sh, n)
+    bins = O.bin_tiles(o, oc, proj, n, cap=max(1, n * 40))
+    t1 = time.perf_counter()
+    pairs, gradP = O.render_sample(o, oc, proj, bins, targets, n, tile_stride, train=True, ncams=len(cams))
+    t2 = time.perf_counter()
+    gradCam = np.zeros((len(cams) + 1) * 8, np.int32)
+    gF, sG = O.chain(o, oc, params, proj, sh, n, gradP, gradCam)
+    m = np.zeros_like(params)
+    v = np.zeros_like(params)
+    sm = np.zeros_like(sh)
+    sv = np.zeros_like(sh)
+    hp = O.adam_hp([1e-4] * 14 + [0, 0], 2001, -9.2, -3.0)
+    O.adam(hp, n, K, params.copy(), gF, m, v, sh.copy(), sG, sm, sv)
+    t3 = time.perf_counter()
+    fixed = (t1 - t0) + (t3 - t2)
+    raster_full = (t2 - t1) * tile_stride
+    return dict(seconds=fixed + raster_full, fixed=fixed, raster_sample=t2 - t1, tile_stride=tile_stride,
+                sample_pairs=pairs)
+
+
+def cpu_targets(args, params, sh, cams, tile_stride):
+    """Targets for the CPU arm (same recipe as the GPU arm: a perturbed copy
+    rendered forward), only for the sampled tiles of camera 0."""
+    from oracle import oracle as O
+    from splat_b200 import scene
+    n = len(params) // 16
+    pp, ps = scene.perturb(params, sh, 0.02, seed=args.seed + 1)
+    total = sum(c["w"] * c["h"] for c in cams)
+    offsets, acc = [], 0
+    for c in cams:
+        offsets.append(acc)
+        acc += c["w"] * c["h"]
+    targets = np.zeros(total, np.uint32)
+    o = O.opts(shDeg=2, entriesCap=max(12_000_000, n * 24))
+    c = cams[0]
+    oc = O.cam(c["R"], c["t"], c["f"], c["cx"], c["cy"], c["w"], c["h"], activeSh=2.0, train=0)
+    proj = O.project(o, oc, pp, ps, n)
+    bins = O.bin_tiles(o, oc, proj, n, cap=max(1, n * 40))
+    img = O.render(o, oc, proj, bins, targets, n, train=False)["img"].reshape(-1, 4)
+    rgb = np.clip(img[:, :3], 0, 1)
+    q = np.minimum(255, np.floor(rgb.astype(np.float64) * 255 + 0.5)).astype(np.uint32)
+    targets[:c["w"] * c["h"]] = (255 << 24) | (q[:, 2] << 16) | (q[:, 1] << 8) | q[:, 0]
+    return targets, offsets
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    O.build()
+    params, sh, cams = workload(args)
+    cores = os.cpu_count() or 1
+    stride = 32
+    targets, offsets = cpu_targets(args, params, sh, cams, stride)
+    times = []
+    for k in range(args.warmup + args.steps):
+        r = cpu_view_sample(args, params, sh, cams, targets, offsets, ci=0, tile_stride=stride)
+        if k >= args.warmup:
+            times.append(r["seconds"])
+    sec = sum(times) / max(1, len(times))
+    v = 1.0 / sec
+    sample = f"each step: one {args.width}x{args.height} view of camera 0; project/bin/chain/Adam over all " \
+             f"{args.splats} splats, raster on every {stride}th tile scaled by {stride}"
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "views/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded surface scene)",
+            "config": config_dict(args, {"parallelism": "host threads"}),
+            "cpu_baseline": {"value": v, "unit": "views/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "views/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from splat_b200 import native as N
+    from splat_b200 import scene
+    from splat_b200.trainer import GSTrainer
+
+    params, sh, cams = workload(args)
+    n = args.splats
+    B = args.batch
+    # config-3 style uneven batch, appended as cameras 24..31
+    uneven_res = [(640, 360), (960, 540), (1280, 720), (1280, 720), (1600, 900), (1920, 1080), (1920, 1080),
+                  (1920, 1080)]
+    extra = []
+    for k, (w, h) in enumerate(uneven_res):
+        cc = scene.ring_cameras(len(uneven_res), 4.0, 0.5, w, h, phase=0.13)[k]
+        cc["imgIdx"] = len(cams) + k
+        extra.append(cc)
+    allcams = cams + extra
+    opts = dict(shDeg=2, maxSplats=n, maxBatch=max(B, len(uneven_res)), batchDepth=args.batch_depth,
+                device=local, persistent=1, useGraphs=1)
+    # targets: render the perturbed scene with the same library, then train the clean one
+    pp, ps = scene.perturb(params, sh, 0.02, seed=args.seed + 1)
+    blank = [dict(tw=c["w"], th=c["h"], rgb=np.zeros(c["w"] * c["h"] * 3, np.float32)) for c in allcams]
+    t = GSTrainer.create(opts)
+    t.setup(dict(data=pp, n=n, sh=ps), allcams, blank, args.width, args.height, 4.0)
+    images = []
+    for c in allcams:
+        img = t.renderView(c)
+        images.append(dict(tw=c["w"], th=c["h"], rgb=np.ascontiguousarray(np.clip(img[..., :3], 0, 1).reshape(-1))))
+    t.setup(dict(data=params, n=n, sh=sh), allcams, images, args.width, args.height, 4.0)
+    del images
+    stream = torch.cuda.Stream(device=local)
+    N.check(N.lib().gs_set_stream(t._h, C.c_void_p(stream.cuda_stream)), t._h)
+    L = N.lib()
+    h = t._h
+
+    def batch_cams(k):
+        return [(k * B + j) % len(cams) for j in range(B)]
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    def timed(fn, steps, views_per_step):
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(steps):
+            fn(k)
+        e1.record(stream)
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if dist:
+            tt = torch.tensor([ms], device=f"cuda:{local}")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+        return ms, views_per_step * steps * world / (ms / 1e3)
+
+    arrs = {}
+
+    def step_batched(k):
+        cs = batch_cams(k)
+        key = tuple(cs)
+        if key not in arrs:
+            arrs[key] = (C.c_uint32 * len(cs))(*cs)
+        N.check(L.gs_step_batch(h, arrs[key], len(cs)), h)
+
+    def step_plain(k):
+        N.check(L.gs_step(h, k % len(cams)), h)
+
+    uneven_idx = (C.c_uint32 * len(extra))(*range(len(cams), len(allcams)))
+
+    def step_uneven(k):
+        N.check(L.gs_step_batch(h, uneven_idx, len(extra)), h)
+
+    t.iter = 2000
+    # ---- plain per-view step (the reference's stepOnce) ----
+    for k in range(args.warmup):
+        step_plain(k)
+    plain_ms, plain_vps = timed(step_plain, args.steps, 1)
+    # ---- batched step (headline) ----
+    for k in range(args.warmup):
+        step_batched(k)
+    with ClockSampler(local) as clk:
+        batch_ms, batch_vps = timed(step_batched, args.steps, B)
+    clocks = clk.summary()
+    # ---- uneven-resolution batch (config 3) ----
+    for k in range(args.warmup):
+        step_uneven(k)
+    uneven_ms, uneven_vps = timed(step_uneven, args.steps, len(extra))
+    # ---- end to end through the public API: per step the camera/Adam records
+    # go host->device from pinned memory and the loss statistics come back ----
+    st = (C.c_uint32 * 4)()
+
+    def step_e2e(k):
+        step_batched(k)
+        N.check(L.gs_read_stats(h, st), h)
+    for k in range(args.warmup):
+        step_e2e(k)
+    e2e_ms, e2e_vps = timed(step_e2e, args.steps, B)
+    # ---- per-phase profile of the batched step (CUDA events on the stream) ----
+    prof_steps = min(args.steps, 5)
+    N.check(L.gs_profile(h, 1), h)
+    for k in range(prof_steps):
+        step_batched(k)
+    ms4 = (C.c_double * 4)()
+    cnt4 = (C.c_uint32 * 4)()
+    N.check(L.gs_profile_read(h, ms4, cnt4), h)
+    N.check(L.gs_profile(h, 0), h)
+    phase = {nm: ms4[i] / max(1, cnt4[i]) for i, nm in enumerate(["project_bin", "sort", "raster", "chain_adam"])}
+    # pairs of one batch (for the raster roofline): sum of per-pixel end indices
+    pairs = 0
+    for k in range(prof_steps):
+        cs = batch_cams(k)
+        arr = (C.c_uint32 * len(cs))(*cs)
+        N.check(L.gs_raster_pass(h, arr, len(cs), 3), h)
+        for v, ci in enumerate(cs):
+            w, hh = allcams[ci]["w"], allcams[ci]["h"]
+            end = np.zeros(w * hh, np.uint32)
+            N.check(L.gs_debug_pixels(h, v, None, None, N.ptr(end, C.c_uint32)), h)
+            pairs += int(end.astype(np.uint64).sum())
+            N.check(L.gs_debug_gradp(h, v, None, 1), h)   # leave no gradients behind
+    pairs_per_launch = pairs / prof_steps
+    peak = C.c_double()
+    N.check(L.gs_probe_fp32_peak(local, C.byref(peak)), None)
+    raster_ms = phase["raster"]
+    achieved = pairs_per_launch * FLOP_PER_PAIR / (raster_ms * 1e-3) / 1e12
+    state = N.GsState()
+    L.gs_get_state(h, C.byref(state))
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            cpu = cpu_baseline_line(args, params, sh, cams)
+        h2d = int(state.stepUploadBytes)  # view records + Adam parameters, from pinned memory
+        line = {"metric": METRIC, "value": batch_vps, "unit": "views/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": batch_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic: seeded surface scene, targets rendered from a perturbed copy",
+                "config": config_dict(args, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                                             "graphs": True, "batch_depth": args.batch_depth}),
+                "plain_step": {"views_per_s": plain_vps, "ms_per_step": plain_ms / args.steps},
+                "batched_vs_plain": batch_vps / plain_vps,
+                "uneven_batch": {"views": [f"{w}x{hh}" for w, hh in uneven_res], "views_per_s": uneven_vps,
+                                 "ms_per_step": uneven_ms / args.steps},
+                "e2e": {"value": e2e_vps, "unit": "views/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 16},
+                "gpu_launches": None,
+                "phases_ms_per_step": phase,
+                "pairs_per_step": pairs_per_launch,
+                "roofline": {"bound": "fp32", "kernel": "raster (fused forward + loss + backward)",
+                             "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                             "frac": achieved / peak.value if peak.value else None, "traffic": None,
+                             "peak_source": "gs_probe_fp32_peak FFMA kernel on this GPU (measured)",
+                             "work": f"{FLOP_PER_PAIR} flop per evaluated pixel-entry pair"},
+                "clocks": clocks,
+                "cpu_baseline": cpu}
+        line["gpu_launches"] = launches_per_step(args.batch) * args.steps
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def launches_per_step(V):
+    # project, tile ranges, splat counts, 3 scan kernels, keygen, radix histogram,
+    # 6 onesweep passes (1080p, <= 2^16 tiles), work order, raster, chain+Adam
+    return 1 + 1 + 1 + 3 + 1 + 1 + 6 + 1 + 1 + 1
+
+
+def cpu_baseline_line(args, params, sh, cams):
+    try:
+        from oracle import oracle as O
+        O.build()
+        stride = 32
+        targets, offsets = cpu_targets(args, params, sh, cams, stride)
+        r = cpu_view_sample(args, params, sh, cams, targets, offsets, ci=0, tile_stride=stride)
+        return {"value": 1.0 / r["seconds"], "unit": "views/s", "cores": os.cpu_count() or 1, "kind": "port",
+                "sample": f"one {args.width}x{args.height} view: project/bin/chain/Adam over all splats, raster on "
+                          f"every {stride}th tile scaled by {stride} ({r['seconds']:.1f} s/view estimated)"}
+    except Exception as e:  # the baseline is reported, never required
+        return {"value": None, "unit": "views/s", "cores": os.cpu_count() or 1, "kind": "port",
+                "sample": f"failed: {e}"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

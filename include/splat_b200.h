@@ -52,13 +52,14 @@ typedef struct gs_options {
   int32_t tileGrad;    /* opts.tileGrad (trainer.js:26): accepted; gradients are identical either way */
   uint64_t entriesCap; /* opts.entriesCap; 0 = reference default (trainer.js:48-49) */
   uint32_t maxSplats;  /* opts.maxSplats; 0 = unset (cap limit 600000, trainer.js:105-107) */
-  float capMult;       /* opts.capMult, default 4 (trainer.js:106) */
   uint32_t maxIters;   /* opts.maxIters: schedule horizon, default 60000 (trainer.js:319) */
-  float minScale;      /* opts.minScale, default 1e-4 (trainer.js:338) */
+  /* options the reference uses in double arithmetic on the host */
+  double capMult;      /* opts.capMult, default 4 (trainer.js:106) */
+  double minScale;     /* opts.minScale, default 1e-4 (trainer.js:338) */
+  double growRate;     /* opts.growRate, default 0.15 (trainer.js:763) */
+  double growUntil;    /* opts.growUntil; negative = 0.75 * horizon (trainer.js:762) */
   float opacityReg;    /* opts.opacityReg, default 0.01 (trainer.js:341) */
   float shLr;          /* opts.shLr, default 1.25e-4 (trainer.js:302) */
-  float growRate;      /* opts.growRate, default 0.15 (trainer.js:763) */
-  float growUntil;     /* opts.growUntil; negative = 0.75 * horizon (trainer.js:762) */
   /* B200 options (no reference counterpart) */
   int32_t tile;            /* raster tile edge in pixels; 16 */
   int32_t batchDepth;      /* splat records staged per shared-memory batch: 32, 64, 128 or 256 */
@@ -77,7 +78,7 @@ typedef struct gs_camera {
   float f, cx, cy;
   int32_t w, h;   /* training resolution */
   int32_t imgIdx; /* index into setup's images[] */
-  float g, b;
+  double g, b;    /* log exposure gain and bias (JavaScript numbers) */
 } gs_camera;
 
 /* One training image of setup's images[] (trainer.js:98): tw*th RGB f32,
@@ -95,6 +96,7 @@ typedef struct gs_state {
   uint64_t entriesCap;
   uint32_t horizon;
   uint32_t lastEntries;   /* kept (tile, splat) entries of the most recent raster */
+  uint32_t stepUploadBytes; /* host->device bytes one step copies (view records + Adam parameters) */
 } gs_state;
 
 /* refine() result (trainer.js:695, 793). early = the donors<16 return. */
@@ -121,7 +123,7 @@ GS_API int gs_abi_version(void);
  * are). */
 GS_API int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, const gs_camera* cams,
              uint32_t ncams, const gs_image* images, uint32_t nimages, uint32_t maxViewW, uint32_t maxViewH,
-             float sceneRadius);
+             double sceneRadius);
 GS_API int gs_get_state(const gs_trainer* h, gs_state* out);
 /* trainer.iter / trainer.horizon / trainer.growLimit writes (session.js:348-349, app.js). */
 GS_API int gs_set_iter(gs_trainer* h, uint32_t iter);

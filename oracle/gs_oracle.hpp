@@ -587,13 +587,15 @@ inline bool lossPixel(const Cam& c, const uint32_t* targets, uint32_t pi, const 
 // forward's T before each entry is kept and the backward reads it).
 template <class T, class Acc>
 void renderView(const Opts& o, const Cam& c, const T* proj, const Bins& b, const uint32_t* targets,
-                float* outImg, PixelState* pxs, Acc acc, bool train, int variant, uint64_t* pairsOut) {
+                float* outImg, PixelState* pxs, Acc acc, bool train, int variant, uint64_t* pairsOut,
+                int tileStride = 1) {
   const int tile = o.tile;
   const int tx = tilesX(c, tile);
   const T E_CUT = T(o.eCut), A_MIN = T(o.aMin);
   uint64_t pairs = 0;
+  if (tileStride < 1) tileStride = 1;
 #pragma omp parallel for schedule(dynamic, 1) reduction(+ : pairs)
-  for (int t = 0; t < b.numTiles; ++t) {
+  for (int t = 0; t < b.numTiles; t += tileStride) {
     const uint32_t s0 = b.start[t], s1 = b.start[t + 1];
     const int ox = (t % tx) * tile, oy = (t / tx) * tile;
     std::vector<T> Tstore;

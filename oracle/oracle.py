@@ -79,6 +79,8 @@ def lib():
                                      u8p, u32p]
         L.oracle_render_f32.argtypes = [P(OOpts), P(OCam), f32p, u32p, u32p, u32p, f32p, f32p, u32p, i32p, u32p,
                                         i32p, u64p, C.c_int, C.c_int]
+        L.oracle_render_sample_f32.argtypes = [P(OOpts), P(OCam), f32p, u32p, u32p, u32p, i32p, u32p, i32p, u64p,
+                                               C.c_int, C.c_int]
         L.oracle_chain_f32.argtypes = [P(OOpts), P(OCam), f32p, f32p, f32p, C.c_uint32, i32p, f32p, f32p, i32p]
         L.oracle_adam_f32.argtypes = [P(OAdam), C.c_uint32, C.c_int, f32p, f32p, f32p, f32p, f32p, f32p, f32p,
                                       f32p]
@@ -239,3 +241,22 @@ def refine(n, cap, params, m, v, sh, shM, shV, K, rng, iter_, growUntil, growRat
                         _p(sh if K else dummy, C.c_float), _p(shM if K else dummy, C.c_float),
                         _p(shV if K else dummy, C.c_float), cb, None, C.byref(out))
     return dict(moved=out.moved, grown=out.grown, n=out.n, early=bool(out.early))
+
+
+def render_sample(o, c, proj, bins, targets, n, tile_stride, train=True, ncams=1):
+    """Raster of every `tile_stride`-th tile (CPU-baseline sampling); returns the pair count."""
+    gradP = np.zeros(n * 16, np.int32)
+    stats = np.zeros(4, np.uint32)
+    gradCam = np.zeros((ncams + 1) * 8, np.int32)
+    pairs = C.c_uint64(0)
+    lib().oracle_render_sample_f32(C.byref(o), C.byref(c), _p(proj, C.c_float), _p(bins["start"], C.c_uint32),
+                                   _p(bins["ids"], C.c_uint32), _p(targets, C.c_uint32), _p(gradP, C.c_int32),
+                                   _p(stats, C.c_uint32), _p(gradCam, C.c_int32), C.byref(pairs), int(train),
+                                   int(tile_stride))
+    return pairs.value, gradP
+
+
+def adam(hp, n, K, params, gradF, m, v, sh, shGrad, shM, shV):
+    lib().oracle_adam_f32(C.byref(hp), n, K, _p(params, C.c_float), _p(gradF, C.c_float), _p(m, C.c_float),
+                          _p(v, C.c_float), _p(sh, C.c_float), _p(shGrad, C.c_float), _p(shM, C.c_float),
+                          _p(shV, C.c_float))

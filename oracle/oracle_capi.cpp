@@ -157,6 +157,19 @@ void oracle_render_f32(const OOpts* oo, const OCam* oc, const float* proj, const
   }
 }
 
+// Render of every tileStride-th tile only (a bounded sample of a view for
+// the CPU baseline's timing; tile work is independent per tile).
+void oracle_render_sample_f32(const OOpts* oo, const OCam* oc, const float* proj, const uint32_t* start,
+                              const uint32_t* ids, const uint32_t* targets, int32_t* gradP, uint32_t* stats,
+                              int32_t* gradCam, uint64_t* pairs, int train, int tileStride) {
+  const Opts o = toOpts(oo);
+  const Cam c = toCam(oc);
+  Bins b = binsFromArrays(o, c, start, ids);
+  std::vector<PixelState> px((size_t)c.W * c.H);
+  AccFixed acc{gradP, stats, gradCam};
+  renderView<float, AccFixed>(o, c, proj, b, targets, nullptr, px.data(), acc, train != 0, 0, pairs, tileStride);
+}
+
 // ---- chain (shaders.js:704-949): consumes and zeroes gradP ----
 void oracle_chain_f32(const OOpts* oo, const OCam* oc, const float* params, const float* proj, const float* sh,
                       uint32_t n, int32_t* gradP, float* gradF, float* shGrad, int32_t* gradCam) {

@@ -59,7 +59,7 @@ struct gs_trainer {
   // ---- host state (GSTrainer fields) ----
   uint32_t n = 0, cap = 0, K = 0, ncams = 0, iter = 0, horizon = 60000, growLimit = 0;
   uint64_t pixelsSeen = 0, entriesCap = 12000000ull, overflowTiles = 0;
-  float sceneRadius = 1.0f;
+  double sceneRadius = 1.0;
   double basePosLr = 0.0;
   float lrs[16] = {};
   float minLS = 0, maxLS = 0;
@@ -180,8 +180,8 @@ static DevCam make_cam(const gs_trainer* h, const gs_camera& c, int train, uint3
   for (int k = 0; k < 3; ++k) { d.t[k] = c.t[k]; d.bg[k] = 0.0f; }
   d.nearz = 0.05f;
   d.f = c.f; d.cx = c.cx; d.cy = c.cy;
-  d.gain = (float)std::exp((double)c.g);
-  d.bias = c.b;
+  d.gain = (float)std::exp(c.g);
+  d.bias = (float)c.b;
   d.activeSh = activeSh;
   d.W = c.w; d.H = c.h;
   d.tilesX = (int)ceil_div((uint32_t)c.w, 16);
@@ -208,13 +208,13 @@ int gs_default_options(gs_options* o) {
   o->tileGrad = 1;
   o->entriesCap = 0;
   o->maxSplats = 0;
-  o->capMult = 4.0f;
+  o->capMult = 4.0;
   o->maxIters = 60000;
-  o->minScale = 1e-4f;
+  o->minScale = 1e-4;
   o->opacityReg = 0.01f;
   o->shLr = 1.25e-4f;
-  o->growRate = 0.15f;
-  o->growUntil = -1.0f;
+  o->growRate = 0.15;
+  o->growUntil = -1.0;
   o->tile = 16;
   o->batchDepth = 64;
   o->maxBatch = 8;
@@ -280,7 +280,7 @@ void gs_destroy(gs_trainer* h) {
 
 int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, const gs_camera* cams,
              uint32_t ncams, const gs_image* images, uint32_t nimages, uint32_t maxViewW, uint32_t maxViewH,
-             float sceneRadius) {
+             double sceneRadius) {
   if (!h) return GS_E_INVALID;
   if (!params || n == 0 || !cams || ncams == 0 || !images) return fail(h, GS_E_INVALID, "setup: empty input");
   cudaSetDevice(h->device);
@@ -411,7 +411,7 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   const float lr[16] = {(float)h->basePosLr, (float)h->basePosLr, (float)h->basePosLr, 5e-3f, 5e-3f, 5e-3f,
                         1e-3f, 1e-3f, 1e-3f, 1e-3f, 1.5e-2f, 1.5e-2f, 1.5e-2f, 2.5e-2f, 0.0f, 0.0f};
   std::memcpy(h->lrs, lr, sizeof(lr));
-  h->minLS = (float)std::log(r * (double)(o.minScale > 0 ? o.minScale : 1e-4f));
+  h->minLS = (float)std::log(r * (o.minScale > 0 ? o.minScale : 1e-4));
   h->maxLS = (float)std::log(r * 0.05);
   h->iter = 0;
   h->pixelsSeen = 0;
@@ -439,6 +439,7 @@ int gs_get_state(const gs_trainer* h, gs_state* out) {
   uint32_t le = 0;
   if (h->ready) cudaMemcpy(&le, h->small + 2057, 4, cudaMemcpyDeviceToHost);
   out->lastEntries = le;
+  out->stepUploadBytes = (uint32_t)sizeof(StepParams);
   return GS_OK;
 }
 
@@ -1114,10 +1115,10 @@ int gs_refine(gs_trainer* h, gs_rng_fn rng, void* ctx, gs_refine_result* out) {
   const uint32_t moved = std::min(nDead, moveCap);
   const uint32_t L = std::min<uint32_t>(nDonors, std::max<uint32_t>(16u, nDonors >> 2));
   const uint32_t limit = std::min(cap, h->growLimit ? h->growLimit : cap);
-  const double growUntil = h->o.growUntil >= 0.0f ? (double)h->o.growUntil : 0.75 * h->horizon;
+  const double growUntil = h->o.growUntil >= 0.0 ? h->o.growUntil : 0.75 * h->horizon;
   uint32_t grown = 0;
   if ((double)h->iter < growUntil) {
-    const double want = std::ceil((double)n * (double)h->o.growRate);
+    const double want = std::ceil((double)n * h->o.growRate);
     grown = (uint32_t)std::max(0.0, std::min(want, (double)limit - (double)n));
   }
   std::vector<uint32_t> big(L);

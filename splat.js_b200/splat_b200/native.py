@@ -20,17 +20,17 @@ ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", 
 class GsOptions(C.Structure):
     _fields_ = [("eCut", C.c_float), ("aMin", C.c_float), ("radClamp", C.c_float), ("anisoReg", C.c_float),
                 ("shDeg", C.c_int32), ("tileGrad", C.c_int32), ("entriesCap", C.c_uint64),
-                ("maxSplats", C.c_uint32), ("capMult", C.c_float), ("maxIters", C.c_uint32),
-                ("minScale", C.c_float), ("opacityReg", C.c_float), ("shLr", C.c_float), ("growRate", C.c_float),
-                ("growUntil", C.c_float), ("tile", C.c_int32), ("batchDepth", C.c_int32),
+                ("maxSplats", C.c_uint32), ("maxIters", C.c_uint32), ("capMult", C.c_double),
+                ("minScale", C.c_double), ("growRate", C.c_double), ("growUntil", C.c_double),
+                ("opacityReg", C.c_float), ("shLr", C.c_float), ("tile", C.c_int32), ("batchDepth", C.c_int32),
                 ("maxBatch", C.c_int32), ("backwardVariant", C.c_int32), ("persistent", C.c_int32),
                 ("useGraphs", C.c_int32), ("device", C.c_int32)]
 
 
 class GsCamera(C.Structure):
     _fields_ = [("R", C.c_float * 9), ("t", C.c_float * 3), ("f", C.c_float), ("cx", C.c_float),
-                ("cy", C.c_float), ("w", C.c_int32), ("h", C.c_int32), ("imgIdx", C.c_int32), ("g", C.c_float),
-                ("b", C.c_float)]
+                ("cy", C.c_float), ("w", C.c_int32), ("h", C.c_int32), ("imgIdx", C.c_int32), ("g", C.c_double),
+                ("b", C.c_double)]
 
 
 class GsImage(C.Structure):
@@ -41,7 +41,7 @@ class GsState(C.Structure):
     _fields_ = [("iter", C.c_uint32), ("n", C.c_uint32), ("cap", C.c_uint32), ("shDeg", C.c_uint32),
                 ("shK", C.c_uint32), ("stride", C.c_uint32), ("ncams", C.c_uint32), ("maxTiles", C.c_uint32),
                 ("pixelsSeen", C.c_uint64), ("entriesCap", C.c_uint64), ("horizon", C.c_uint32),
-                ("lastEntries", C.c_uint32)]
+                ("lastEntries", C.c_uint32), ("stepUploadBytes", C.c_uint32)]
 
 
 class GsRefineResult(C.Structure):
@@ -72,7 +72,7 @@ def lib():
         "gs_destroy": (None, [H]),
         "gs_last_error": (C.c_char_p, [H]),
         "gs_setup": (C.c_int, [H, f32p, C.c_uint32, f32p, P(GsCamera), C.c_uint32, P(GsImage), C.c_uint32,
-                               C.c_uint32, C.c_uint32, C.c_float]),
+                               C.c_uint32, C.c_uint32, C.c_double]),
         "gs_get_state": (C.c_int, [H, P(GsState)]),
         "gs_set_iter": (C.c_int, [H, C.c_uint32]),
         "gs_set_horizon": (C.c_int, [H, C.c_uint32]),

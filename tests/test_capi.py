@@ -46,8 +46,8 @@ def test_default_options_match_reference():
 
 
 def test_struct_sizes_match_header():
-    # gs_options: 4 f32, 2 i32, u64, u32, f32, u32, 5 f32, 7 i32 -> 80 bytes with padding
-    assert C.sizeof(N.GsCamera) == 4 * (9 + 3 + 3 + 2 + 1 + 2)
+    assert C.sizeof(N.GsOptions) == 4 * 6 + 8 + 4 * 2 + 8 * 4 + 4 * 2 + 4 * 7 + 4
+    assert C.sizeof(N.GsCamera) == 4 * (9 + 3 + 3 + 3) + 8 * 2
     assert C.sizeof(N.GsImage) == 16
     assert C.sizeof(N.GsRefineResult) == 24
 
