@@ -90,7 +90,7 @@ void oracle_project_f64(const OOpts* oo, const OCam* oc, const double* params, c
 }
 
 // Per-splat values the rasteriser reads, derived from proj exactly as the
-// render pass does (w = opa*comp, cnorm = 1/(1+lambda_max)), plus tile
+// render pass does (w = opa*comp, cnorm = 1/(1+lambda_max), cull radius), plus tile
 // bounds packed {x0 | y0<<16, x1 | y1<<16} ({~0, 0} when culled).
 void oracle_records_f32(const OOpts* oo, const OCam* oc, const float* proj, uint32_t n, float* rec12,
                         uint32_t* rect2) {
@@ -105,7 +105,10 @@ void oracle_records_f32(const OOpts* oo, const OCam* oc, const float* proj, uint
       continue;
     }
     const Splat2D<float> s = splat2D<float>(pr);
-    const float v[12] = {s.mx, s.my, s.cA, s.cB, s.cC, s.w, s.r, s.g, s.b, s.opa, s.cnorm, pr[2]};
+    // the rasteriser's conservative whole-warp cull radius: rad + 1 px, or
+    // unbounded when the radius clamp (radClamp * W) was active
+    const float cullR = pr[15] >= o.radClamp * (float)c.W ? INFINITY : pr[15] + 1.0f;
+    const float v[12] = {s.mx, s.my, s.cA, s.cB, s.cC, s.w, s.r, s.g, s.b, s.opa, s.cnorm, cullR};
     for (int k = 0; k < 12; ++k) r[k] = v[k];
     const TileRect t = tileRect<float>(c, o.tile, pr[0], pr[1], pr[15]);
     rect2[2 * i] = (uint32_t)t.x0 | ((uint32_t)t.y0 << 16);

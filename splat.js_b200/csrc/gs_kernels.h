@@ -17,6 +17,7 @@ struct ProjectArgs {
   float eCut, aMin, radClamp;
   int tile;
   RenderRec* recs;         // V * n
+  float* depth;            // V * n camera-space depth (sort key)
   uint2* rect;             // V * n
   int32_t* diffGrid;       // per view (tilesX+1)*(tilesY+1), cleared before
   const uint32_t* gridBase;  // V offsets into diffGrid
@@ -51,7 +52,7 @@ struct KeygenArgs {
   int V;
   const DevCam* cams;
   const uint2* rect;
-  const RenderRec* recs;
+  const float* depth;
   const uint8_t* dropped;
   const uint32_t* viewDrops;
   const uint32_t* offsets;  // V * n exclusive scan of counts

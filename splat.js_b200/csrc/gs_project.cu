@@ -78,11 +78,16 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   const float lmax = mid + disc;
   const float cnorm = 1.0f / (1.0f + lmax);
 
+  // conservative cull radius for whole warps of pixels: beyond `rad` from the
+  // mean no pixel passes both cutoffs (e >= d^2 / (2 lambda_max) > eMax),
+  // unless the radius was clamped; one pixel of margin covers rounding
+  const float cullR = rad >= a.radClamp * (float)c.W ? __int_as_float(0x7F800000) : rad + 1.0f;
   RenderRec r;
   r.r0 = make_float4(mx, my, cd * inv, -g.vb * inv);
   r.r1 = make_float4(ad * inv, opa * comp, col[0], col[1]);
-  r.r2 = make_float4(col[2], opa, cnorm, g.pc[2]);
+  r.r2 = make_float4(col[2], opa, cnorm, cullR);
   a.recs[slot] = r;
+  a.depth[slot] = g.pc[2];
 
   // tile bounds (shaders.js:303-308)
   const int tx = c.tilesX, ty = c.tilesY;
@@ -242,7 +247,7 @@ __global__ void __launch_bounds__(256) k_keygen(KeygenArgs a) {
   const uint32_t i = (uint32_t)(gid - (uint64_t)v * a.n);
   const DevCam& c = a.cams[v];
   const uint32_t x0 = r.x & 0xFFFFu, y0 = r.x >> 16, x1 = r.y & 0xFFFFu, y1 = r.y >> 16;
-  const uint32_t depthBits = __float_as_uint(a.recs[gid].r2.w);
+  const uint32_t depthBits = __float_as_uint(a.depth[gid]);
   const uint8_t* dr = a.dropped + c.tileBase;
   const bool anyDrop = a.viewDrops[v] != 0;
   uint32_t o = a.offsets[gid];

@@ -3,35 +3,39 @@
 // (shaders.js:544-700), over a shared (view, tile) work queue.
 //
 // One CTA works on one 16x16 tile at a time (256 threads, one pixel each;
-// warp w covers an 8x4 block of the tile so a splat's footprint tends to
-// cover whole warps).  Splat records of the tile's sorted entries are staged
-// in shared memory BATCH at a time.
+// warp w covers an 8x4 block of the tile).  Splat records of the tile's
+// sorted entries are staged in shared memory BATCH at a time.
 //
-// Forward: front-to-back compositing; the block leaves the tile as soon as
-// __syncthreads_count (a block-wide ballot) finds every pixel saturated.
-// Backward: each pixel walks its entries back to front from its own end
-// index, recovering the transmittance in front of each splat from the final
-// one (Tb = Ta / (1 - alpha)) -- or, in the stored-state variant, reading
-// the value the forward saved.  Every pixel's ten gradient contributions are
+// Forward: front-to-back compositing.  Before any per-pixel work, a
+// warp-uniform test drops entries whose conservative radius (rad + 1 px; the
+// binning radius bounds where both cutoffs can pass, so no pixel farther
+// away can composite) misses the warp's 8x4 block; the block leaves the tile
+// when __syncthreads_count (a block-wide ballot) finds every pixel saturated.
+// In the fused train kernel each warp also records, per entry, whether any
+// of its pixels composited it (a ballot bit in shared memory).
+// Backward: each warp walks only the entries its bits mark, back to front;
+// each pixel recovers the transmittance in front of a splat from the final
+// one (Tb = Ta / (1 - alpha)) -- or, in the stored-state variant, reads the
+// value the forward saved.  The ten gradient contributions of each pixel are
 // truncated to i32 fixed point (the reference's i32(clamp(v*16384, +-1e9)))
 // and summed exactly: a warp REDUX per slot, a shared-memory add per
 // (entry, slot) across the tile's warps, and one global atomic per (splat,
-// slot, tile).  Integer sums commute, so the result is bit-identical in any
+// slot, tile).  Integer sums commute, so results are bit-identical in any
 // order -- the deterministic mode is the only mode.
 //
-// The per-pair arithmetic is the canonical FP32 sequence (fused where
-// written fmaf) that the CPU restatement performs too.
+// The per-pair arithmetic is the canonical FP32 sequence the CPU
+// restatement performs.  The 2^14 fixed-point scale is folded into upstream
+// factors (galpha, gC): scaling by a power of two is exact, so every
+// truncated integer equals the one the unfolded sequence produces.
 #include "gs_common.cuh"
 #include "gs_kernels.h"
 
 namespace gs {
 
-constexpr int RT = 16;           // tile edge (pixels)
+constexpr int RT = 16;            // tile edge (pixels)
 constexpr int RTHREADS = RT * RT;
-
-struct PixelCtx {
-  float px, py;
-};
+constexpr int MASKW = 128;        // ballot-bit words per warp: entries 0..4095 of a tile
+constexpr uint32_t FULL = 0xFFFFFFFFu;
 
 __device__ __forceinline__ float pairExponent(const float4& r0, float cC, float dx, float dy) {
   // e = max(fma(0.5, fma(cA*dx, dx, (cC*dy)*dy), (cB*dx)*dy), 0)
@@ -39,11 +43,24 @@ __device__ __forceinline__ float pairExponent(const float4& r0, float cC, float 
   return fmaxf(__fmaf_rn(0.5f, q, (r0.w * dx) * dy), 0.0f);
 }
 
+// trunc(clamp(x, -1e9, 1e9)) for an already scaled value
+__device__ __forceinline__ int32_t fix_scaled(float x) { return __float2int_rz(fminf(fmaxf(x, -1.0e9f), 1.0e9f)); }
+
+// warp-uniform: can the splat reach any pixel centre of the warp's 8x4 block?
+__device__ __forceinline__ bool warpTouches(const float4& r0, float cullR, float wcx, float wcy) {
+  const float ox = fmaxf(fabsf(r0.x - wcx) - 3.5f, 0.0f);
+  const float oy = fmaxf(fabsf(r0.y - wcy) - 1.5f, 0.0f);
+  return ox * ox + oy * oy <= cullR * cullR;
+}
+
 template <int BATCH, bool FWD, bool BWD, bool STORED>
 __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
+  constexpr bool MASKS = FWD && BWD;
+  static_assert(BATCH % 32 == 0, "batches hold whole ballot words");
   __shared__ RenderRec s_rec[BATCH];
   __shared__ uint32_t s_id[BATCH];
   __shared__ int32_t s_acc[BWD ? BATCH * 10 : 1];
+  __shared__ uint32_t s_mask[MASKS ? 8 * MASKW : 1];
   __shared__ uint32_t s_item;
   __shared__ uint32_t s_redu[8][5];
   __shared__ uint32_t s_endmax[8];
@@ -52,19 +69,15 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
   const int lx = ((wid & 1) << 3) | (lane & 7);
   const int ly = ((wid >> 1) << 2) | (lane >> 3);
   const float E_CUT = a.eCut, A_MIN = a.aMin;
+  uint32_t* wmask = s_mask + (MASKS ? wid * MASKW : 0);
 
   if (BWD)
     for (int k = tid; k < BATCH * 10; k += RTHREADS) s_acc[k] = 0;
 
   for (uint32_t iter = 0;; ++iter) {
     // ---- next work item (a global tile of the batch) ----
-    if (a.workCounter) {
-      if (tid == 0) s_item = atomicAdd(a.workCounter, 1u);
-      __syncthreads();
-    } else {
-      if (tid == 0) s_item = iter == 0 ? blockIdx.x : 0xFFFFFFFFu;
-      __syncthreads();
-    }
+    if (tid == 0) s_item = a.workCounter ? atomicAdd(a.workCounter, 1u) : (iter == 0 ? blockIdx.x : 0xFFFFFFFFu);
+    __syncthreads();
     const uint32_t item = s_item;
     __syncthreads();
     if (item >= a.totalTiles) break;
@@ -77,6 +90,9 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
     const int x = tx * RT + lx, y = ty * RT + ly;
     const bool inside = x < c.W && y < c.H;
     const float px = (float)x + 0.5f, py = (float)y + 0.5f;
+    // centre of the warp's pixel centres (8 wide, 4 high)
+    const float wcx = (float)(tx * RT + ((wid & 1) << 3)) + 4.0f;
+    const float wcy = (float)(ty * RT + ((wid >> 1) << 2)) + 2.0f;
     const uint2 rg = a.ranges[gt];
     const uint32_t s = rg.x, e = rg.y;
     const size_t pix = (size_t)c.pixBase + (size_t)y * c.W + x;
@@ -84,9 +100,13 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
 
     float T = 1.0f;
     float C0 = 0.0f, C1 = 0.0f, C2 = 0.0f;
-    uint32_t cnt = 0;
+    uint32_t cnt = e - s;  // one past the last processed entry (relative)
     if (FWD) {
       bool done = !inside;
+      if (MASKS) {
+        for (int k = lane; k < MASKW; k += 32) wmask[k] = 0u;
+        __syncwarp();
+      }
       for (uint32_t base = s; base < e; base += BATCH) {
         if (__syncthreads_count(!done) == 0) break;
         const uint32_t nb = min((uint32_t)BATCH, e - base);
@@ -96,25 +116,41 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
           s_rec[k] = recs[id];
         }
         __syncthreads();
-        if (!done) {
+        if (!__all_sync(FULL, done)) {
+          const uint32_t rbase = base - s;
+          uint32_t bits = 0;
           for (uint32_t j = 0; j < nb; ++j) {
             const float4 r0 = s_rec[j].r0;
-            const float4 r1 = s_rec[j].r1;
-            const float dx = px - r0.x, dy = py - r0.y;
-            const float ee = pairExponent(r0, r1.x, dx, dy);
-            cnt = base - s + j + 1;
-            if (ee > E_CUT) continue;
-            const float araw = r1.y * gexp(-ee);
-            const float alpha = fminf(0.99f, araw);
-            if (alpha < A_MIN) continue;
-            if (STORED) a.tStore[(size_t)(base + j) * RTHREADS + tid] = T;
-            const float ta = T * alpha;
-            const float cb = s_rec[j].r2.x;
-            C0 = __fmaf_rn(ta, r1.z, C0);
-            C1 = __fmaf_rn(ta, r1.w, C1);
-            C2 = __fmaf_rn(ta, cb, C2);
-            T = T * (1.0f - alpha);
-            if (T < 1e-4f) { done = true; break; }
+            bool contrib = false;
+            if (warpTouches(r0, s_rec[j].r2.w, wcx, wcy)) {
+              if (!done) {
+                const float4 r1 = s_rec[j].r1;
+                const float dx = px - r0.x, dy = py - r0.y;
+                const float ee = pairExponent(r0, r1.x, dx, dy);
+                if (ee <= E_CUT) {
+                  const float araw = r1.y * gexp(-ee);
+                  const float alpha = fminf(0.99f, araw);
+                  if (alpha >= A_MIN) {
+                    contrib = true;
+                    if (STORED) a.tStore[(size_t)(base + j) * RTHREADS + tid] = T;
+                    const float ta = T * alpha;
+                    C0 = __fmaf_rn(ta, r1.z, C0);
+                    C1 = __fmaf_rn(ta, r1.w, C1);
+                    C2 = __fmaf_rn(ta, s_rec[j].r2.x, C2);
+                    T = T * (1.0f - alpha);
+                    if (T < 1e-4f) { done = true; cnt = rbase + j + 1; }
+                  }
+                }
+              }
+              if (MASKS && __ballot_sync(FULL, contrib)) bits |= 1u << (j & 31);
+            }
+            const bool allDone = __all_sync(FULL, done);
+            if (MASKS && ((j & 31) == 31 || j + 1 == nb || allDone)) {
+              const uint32_t w = (rbase + j) >> 5;
+              if (lane == 0 && w < MASKW) wmask[w] = bits;
+              bits = 0;
+            }
+            if (allDone) break;
           }
         }
         __syncthreads();
@@ -137,6 +173,7 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
     if (BWD) {
       // ---- loss (shaders.js:589-618) ----
       bool lossOk = false;
+      float g16_0 = 0.0f, g16_1 = 0.0f, g16_2 = 0.0f;  // gC * 2^14
       float gC0 = 0.0f, gC1 = 0.0f, gC2 = 0.0f;
       uint32_t st0 = 0, st1 = 0, st2 = 0;
       int32_t cg6 = 0, cg7 = 0;
@@ -158,6 +195,7 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
           const float rt0 = sqrtf(er0 * er0 + D2), rt1 = sqrtf(er1 * er1 + D2), rt2 = sqrtf(er2 * er2 + D2);
           const float eg0 = er0 / rt0, eg1 = er1 / rt1, eg2 = er2 / rt2;
           gC0 = gain * eg0; gC1 = gain * eg1; gC2 = gain * eg2;
+          g16_0 = gC0 * FIXED; g16_1 = gC1 * FIXED; g16_2 = gC2 * FIXED;
           const float lossv = (rt0 + rt1 + rt2) - 8.9999999999999997e-02f;  // f32(3 * 0.03)
           st1 = u32sat(lossv * 32768.0f);
           cg6 = fixq((eg0 * C0 + eg1 * C1 + eg2 * C2) * gain, FIXCAM);
@@ -168,12 +206,12 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
       // reference's atomics) and the largest end index of the tile
       const uint32_t myEnd = lossOk ? cnt : 0u;
       {
-        const uint32_t r0 = __reduce_add_sync(0xFFFFFFFFu, st0);
-        const uint32_t r1 = __reduce_add_sync(0xFFFFFFFFu, st1);
-        const uint32_t r2 = __reduce_add_sync(0xFFFFFFFFu, st2);
-        const uint32_t r3 = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)cg6);
-        const uint32_t r4 = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)cg7);
-        const uint32_t mx = __reduce_max_sync(0xFFFFFFFFu, myEnd);
+        const uint32_t r0 = __reduce_add_sync(FULL, st0);
+        const uint32_t r1 = __reduce_add_sync(FULL, st1);
+        const uint32_t r2 = __reduce_add_sync(FULL, st2);
+        const uint32_t r3 = __reduce_add_sync(FULL, (uint32_t)cg6);
+        const uint32_t r4 = __reduce_add_sync(FULL, (uint32_t)cg7);
+        const uint32_t mx = __reduce_max_sync(FULL, myEnd);
         if (lane == 0) {
           s_redu[wid][0] = r0; s_redu[wid][1] = r1; s_redu[wid][2] = r2;
           s_redu[wid][3] = r3; s_redu[wid][4] = r4;
@@ -206,15 +244,29 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
           s_rec[k] = recs[id];
         }
         __syncthreads();
-        for (uint32_t jj = nb; jj > 0; --jj) {
-          const uint32_t j = lo + jj - 1;  // relative entry index
+        // this warp's entries in [lo, hi), back to front
+        int32_t jn = (int32_t)hi - 1;
+        while (jn >= (int32_t)lo) {
+          uint32_t j = (uint32_t)jn;
+          if (MASKS && j < (uint32_t)MASKW * 32u) {
+            const uint32_t w = j >> 5;
+            uint32_t word = wmask[w] & (FULL >> (31u - (j & 31u)));
+            if ((w << 5) < lo) word &= ~((1u << (lo & 31u)) - 1u);
+            if (word == 0u) { jn = (int32_t)(w << 5) - 1; continue; }
+            j = (w << 5) + 31u - (uint32_t)__clz(word);
+          } else if (!warpTouches(s_rec[j - lo].r0, s_rec[j - lo].r2.w, wcx, wcy)) {
+            jn = (int32_t)j - 1;
+            continue;
+          }
+          jn = (int32_t)j - 1;
+          const RenderRec& rr = s_rec[j - lo];
           int32_t q[10];
 #pragma unroll
           for (int k = 0; k < 10; ++k) q[k] = 0;
           bool contrib = false;
           if (j < myEnd) {
-            const float4 r0 = s_rec[jj - 1].r0;
-            const float4 r1 = s_rec[jj - 1].r1;
+            const float4 r0 = rr.r0;
+            const float4 r1 = rr.r1;
             const float dx = px - r0.x, dy = py - r0.y;
             const float ee = pairExponent(r0, r1.x, dx, dy);
             if (ee <= E_CUT) {
@@ -223,7 +275,7 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
               const float alpha = fminf(0.99f, araw);
               if (alpha >= A_MIN) {
                 contrib = true;
-                const float4 r2 = s_rec[jj - 1].r2;
+                const float4 r2 = rr.r2;
                 const float inv = __frcp_rn(1.0f - alpha);
                 const float Tb = STORED ? a.tStore[(size_t)(s + j) * RTHREADS + tid] : Ta * inv;
                 const float aT = alpha * Tb;
@@ -232,19 +284,20 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
                 const float g2 = __fmaf_rn(r2.x, Tb, -(S2 * inv));
                 float galpha = __fmaf_rn(gC2, g2, __fmaf_rn(gC1, g1, gC0 * g0));
                 if (araw > 0.99f) galpha = 0.0f;
-                const float ga = galpha * araw;
-                q[0] = fixq(ga * __fmaf_rn(r0.z, dx, r0.w * dy), FIXED);
-                q[1] = fixq(ga * __fmaf_rn(r0.w, dx, r1.x * dy), FIXED);
-                const float gq = ga * (-0.5f * r2.z);
-                const float gqx = gq * dx;
-                q[2] = fixq(gqx * dx, FIXEDC);
-                q[3] = fixq((gqx * dy) * 2.0f, FIXEDC);
-                q[4] = fixq((gq * dy) * dy, FIXEDC);
-                q[5] = fixq((galpha * r2.y) * G, FIXED);
-                q[6] = fixq(ga * (1.0f - r2.y), FIXED);
-                q[7] = fixq(gC0 * aT, FIXED);
-                q[8] = fixq(gC1 * aT, FIXED);
-                q[9] = fixq(gC2 * aT, FIXED);
+                const float gal16 = galpha * FIXED;
+                const float ga16 = gal16 * araw;
+                q[0] = fix_scaled(ga16 * __fmaf_rn(r0.z, dx, r0.w * dy));
+                q[1] = fix_scaled(ga16 * __fmaf_rn(r0.w, dx, r1.x * dy));
+                const float gq16 = ga16 * (-0.5f * r2.z);
+                const float gqx16 = gq16 * dx;
+                q[2] = fix_scaled(gqx16 * dx);
+                q[3] = fix_scaled((gqx16 * dy) * 2.0f);
+                q[4] = fix_scaled((gq16 * dy) * dy);
+                q[5] = fix_scaled((gal16 * r2.y) * G);
+                q[6] = fix_scaled(ga16 * (1.0f - r2.y));
+                q[7] = fix_scaled(g16_0 * aT);
+                q[8] = fix_scaled(g16_1 * aT);
+                q[9] = fix_scaled(g16_2 * aT);
                 S0 = __fmaf_rn(r1.z, aT, S0);
                 S1 = __fmaf_rn(r1.w, aT, S1);
                 S2 = __fmaf_rn(r2.x, aT, S2);
@@ -252,14 +305,14 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
               }
             }
           }
-          if (__any_sync(0xFFFFFFFFu, contrib)) {
+          if (__any_sync(FULL, contrib)) {
             uint32_t r[10];
 #pragma unroll
-            for (int k = 0; k < 10; ++k) r[k] = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)q[k]);
+            for (int k = 0; k < 10; ++k) r[k] = __reduce_add_sync(FULL, (uint32_t)q[k]);
             uint32_t mine = r[0];
 #pragma unroll
             for (int k = 1; k < 10; ++k) mine = lane == k ? r[k] : mine;
-            if (lane < 10 && mine) atomicAdd(&s_acc[(jj - 1) * 10 + lane], (int32_t)mine);
+            if (lane < 10 && mine) atomicAdd(&s_acc[(j - lo) * 10 + lane], (int32_t)mine);
           }
         }
         __syncthreads();

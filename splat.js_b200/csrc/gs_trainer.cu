@@ -72,6 +72,7 @@ struct gs_trainer {
   // ---- device buffers ----
   float *params = nullptr, *m = nullptr, *v = nullptr, *sh = nullptr, *shM = nullptr, *shV = nullptr;
   RenderRec* recs = nullptr;
+  float* depth = nullptr;
   uint2* rect = nullptr;
   uint32_t *counts = nullptr, *offsets = nullptr;
   int32_t* gradP = nullptr;
@@ -354,6 +355,7 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   GS_AL(h->shM, std::max<size_t>(shn, 1));
   GS_AL(h->shV, std::max<size_t>(shn, 1));
   GS_AL(h->recs, (size_t)B * cap);
+  GS_AL(h->depth, (size_t)B * cap);
   GS_AL(h->rect, (size_t)B * cap);
   GS_AL(h->counts, (size_t)B * cap);
   GS_AL(h->offsets, (size_t)B * cap);
@@ -544,6 +546,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   pa.radClamp = h->o.radClamp;
   pa.tile = 16;
   pa.recs = h->recs;
+  pa.depth = h->depth;
   pa.rect = h->rect;
   pa.diffGrid = h->diffGrid;
   pa.gridBase = h->dParams->gridBase;
@@ -579,7 +582,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   ka.V = V;
   ka.cams = dcams;
   ka.rect = h->rect;
-  ka.recs = h->recs;
+  ka.depth = h->depth;
   ka.dropped = h->dropped;
   ka.viewDrops = h->viewDrops;
   ka.offsets = h->offsets;
