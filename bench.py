@@ -70,7 +70,8 @@ def config_dict(args, extra=None):
     d = {"workload": f"{args.splats // 1000}k-splat surface scene, SH deg 2, {args.width}x{args.height}, "
                      f"batch of {args.batch} views per step",
          "splats": args.splats, "resolution": f"{args.width}x{args.height}", "views_per_batched_step": args.batch,
-         "cameras": args.cams, "sh_degree": 2, "tile": 16, "l2": "working set > L2 (no flush needed)"}
+         "cameras": args.cams, "sh_degree": 2, "tile": 16, "l2": "working set > L2 (no flush needed)",
+         "iteration_start": 2000}
     if extra:
         d.update(extra)
     return d
@@ -311,6 +312,8 @@ def run_ours(args):
         N.check(L.gs_step_batch(h, uneven_idx, len(extra)), h)
 
     t.iter = 2000
+    # ---- autotuner: tile size x splat-batch depth on the first batch ----
+    tune_tile, tune_depth, tune_table = t.autotune(batch_cams(0), reps=2)
     # ---- plain per-view step (the reference's stepOnce) ----
     for k in range(args.warmup):
         step_plain(k)
@@ -376,7 +379,8 @@ def run_ours(args):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic: seeded surface scene, targets rendered from a perturbed copy",
                 "config": config_dict(args, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                                             "graphs": True, "batch_depth": args.batch_depth}),
+                                             "graphs": True, "tile": tune_tile, "batch_depth": tune_depth}),
+                "autotune_ms_per_pass": {f"{k[0]}x{k[1]}": round(v, 3) for k, v in tune_table.items()},
                 "plain_step": {"views_per_s": plain_vps, "ms_per_step": plain_ms / args.steps},
                 "batched_vs_plain": batch_vps / plain_vps,
                 "uneven_batch": {"views": [f"{w}x{hh}" for w, hh in uneven_res], "views_per_s": uneven_vps,

@@ -61,8 +61,8 @@ typedef struct gs_options {
   float opacityReg;    /* opts.opacityReg, default 0.01 (trainer.js:341) */
   float shLr;          /* opts.shLr, default 1.25e-4 (trainer.js:302) */
   /* B200 options (no reference counterpart) */
-  int32_t tile;            /* raster tile edge in pixels; 16 */
-  int32_t batchDepth;      /* splat records staged per shared-memory batch: 32, 64, 128 or 256 */
+  int32_t tile;            /* raster tile edge in pixels: 8, 16 (the reference's TILE) or 32 */
+  int32_t batchDepth;      /* splat records staged per shared-memory batch: 64, 128 or 256 */
   int32_t maxBatch;        /* most views one gs_step_batch may take (buffers are sized for it) */
   int32_t backwardVariant; /* 0: recompute transmittance from the final T (reference); 1: stored-state */
   int32_t persistent;      /* 1: raster over a persistent (view, tile) work queue, heaviest tiles first */
@@ -189,6 +189,16 @@ GS_API int gs_profile_read(gs_trainer* h, double ms[4], uint32_t launches[4]);
 /* FP32 FMA throughput of device `device` in TFLOP/s (an FFMA-chain kernel),
  * the peak the raster kernels' roofline is quoted against. */
 GS_API int gs_probe_fp32_peak(int32_t device, double* tflops);
+
+/* ---- raster configuration (no reference counterpart; results do not depend
+ * on it: images and gradients are identical for every tile size and depth,
+ * only the per-tile entry lists follow the tile size) ----
+ * gs_autotune times the training pass on views ci[0..nviews) for each tile
+ * edge {8, 16, 32} x splat-batch depth {64, 128, 256}, keeps the fastest
+ * and reports it; msOut (9 floats, tile-major) may be NULL. */
+GS_API int gs_autotune(gs_trainer* h, const uint32_t* ci, uint32_t nviews, int32_t reps, int32_t* bestTile,
+                       int32_t* bestDepth, float* msOut);
+GS_API int gs_set_raster_config(gs_trainer* h, int32_t tile, int32_t batchDepth);
 
 /* ---- introspection of the most recent raster (parity checks) ----
  * gs_raster_pass runs project -> bin -> raster (no chain, no Adam) on views

@@ -2,18 +2,19 @@
 // the back-to-front backward of the reference's render pass
 // (shaders.js:544-700), over a shared (view, tile) work queue.
 //
-// One CTA works on one 16x16 tile at a time (256 threads, one pixel each;
-// warp w covers an 8x4 block of the tile).  Splat records of the tile's
+// One CTA works on one TILE x TILE tile at a time (TILE = 8, 16 or 32; one
+// thread per pixel; each warp covers an 8x4 block of the tile).  Splat records of the tile's
 // sorted entries are staged in shared memory BATCH at a time.
 //
-// Forward: front-to-back compositing.  Before any per-pixel work, a
-// warp-uniform test drops entries whose conservative radius (rad + 1 px; the
-// binning radius bounds where both cutoffs can pass, so no pixel farther
-// away can composite) misses the warp's 8x4 block; the block leaves the tile
-// when __syncthreads_count (a block-wide ballot) finds every pixel saturated.
-// In the fused train kernel each warp also records, per entry, whether any
-// of its pixels composited it (a ballot bit in shared memory).
-// Backward: each warp walks only the entries its bits mark, back to front;
+// Forward: front-to-back compositing; the block leaves the tile when
+// __syncthreads_count (a block-wide ballot) finds every pixel saturated.  In
+// the fused train kernel each warp also records, per entry, whether any of
+// its pixels composited it (a ballot bit in shared memory): on dense scenes
+// only about a fifth of warp-entries composite anything.
+// Backward: each warp walks only the entries its bits mark, back to front
+// (without bits -- backward from saved state, or entries past the bit
+// capacity -- a warp-uniform test against the splat's conservative radius,
+// rad + 1 px, skips entries that cannot reach the warp's 8x4 pixels);
 // each pixel recovers the transmittance in front of a splat from the final
 // one (Tb = Ta / (1 - alpha)) -- or, in the stored-state variant, reads the
 // value the forward saved.  The ten gradient contributions of each pixel are
@@ -32,8 +33,6 @@
 
 namespace gs {
 
-constexpr int RT = 16;            // tile edge (pixels)
-constexpr int RTHREADS = RT * RT;
 constexpr int MASKW = 128;        // ballot-bit words per warp: entries 0..4095 of a tile
 constexpr uint32_t FULL = 0xFFFFFFFFu;
 
@@ -53,21 +52,26 @@ __device__ __forceinline__ bool warpTouches(const float4& r0, float cullR, float
   return ox * ox + oy * oy <= cullR * cullR;
 }
 
-template <int BATCH, bool FWD, bool BWD, bool STORED>
-__global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
+// TILE x TILE pixels per CTA, one per thread; warps cover 8x4 blocks.
+template <int TILE, int BATCH, bool FWD, bool BWD, bool STORED>
+__global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
+  constexpr int RT = TILE;
+  constexpr int RTHREADS = TILE * TILE;
+  constexpr int NW = RTHREADS / 32;  // warps
+  constexpr int WPR = TILE / 8;      // 8-wide warp blocks per tile row
   constexpr bool MASKS = FWD && BWD;
   static_assert(BATCH % 32 == 0, "batches hold whole ballot words");
   __shared__ RenderRec s_rec[BATCH];
   __shared__ uint32_t s_id[BATCH];
   __shared__ int32_t s_acc[BWD ? BATCH * 10 : 1];
-  __shared__ uint32_t s_mask[MASKS ? 8 * MASKW : 1];
+  __shared__ uint32_t s_mask[MASKS ? NW * MASKW : 1];
   __shared__ uint32_t s_item;
-  __shared__ uint32_t s_redu[8][5];
-  __shared__ uint32_t s_endmax[8];
+  __shared__ uint32_t s_redu[NW][5];
+  __shared__ uint32_t s_endmax[NW];
 
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  const int lx = ((wid & 1) << 3) | (lane & 7);
-  const int ly = ((wid >> 1) << 2) | (lane >> 3);
+  const int lx = (wid % WPR) * 8 + (lane & 7);
+  const int ly = (wid / WPR) * 4 + (lane >> 3);
   const float E_CUT = a.eCut, A_MIN = a.aMin;
   uint32_t* wmask = s_mask + (MASKS ? wid * MASKW : 0);
 
@@ -91,8 +95,8 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
     const bool inside = x < c.W && y < c.H;
     const float px = (float)x + 0.5f, py = (float)y + 0.5f;
     // centre of the warp's pixel centres (8 wide, 4 high)
-    const float wcx = (float)(tx * RT + ((wid & 1) << 3)) + 4.0f;
-    const float wcy = (float)(ty * RT + ((wid >> 1) << 2)) + 2.0f;
+    const float wcx = (float)(tx * RT + (wid % WPR) * 8) + 4.0f;
+    const float wcy = (float)(ty * RT + (wid / WPR) * 4) + 2.0f;
     const uint2 rg = a.ranges[gt];
     const uint32_t s = rg.x, e = rg.y;
     const size_t pix = (size_t)c.pixBase + (size_t)y * c.W + x;
@@ -120,37 +124,36 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
           const uint32_t rbase = base - s;
           uint32_t bits = 0;
           for (uint32_t j = 0; j < nb; ++j) {
-            const float4 r0 = s_rec[j].r0;
             bool contrib = false;
-            if (warpTouches(r0, s_rec[j].r2.w, wcx, wcy)) {
-              if (!done) {
-                const float4 r1 = s_rec[j].r1;
-                const float dx = px - r0.x, dy = py - r0.y;
-                const float ee = pairExponent(r0, r1.x, dx, dy);
-                if (ee <= E_CUT) {
-                  const float araw = r1.y * gexp(-ee);
-                  const float alpha = fminf(0.99f, araw);
-                  if (alpha >= A_MIN) {
-                    contrib = true;
-                    if (STORED) a.tStore[(size_t)(base + j) * RTHREADS + tid] = T;
-                    const float ta = T * alpha;
-                    C0 = __fmaf_rn(ta, r1.z, C0);
-                    C1 = __fmaf_rn(ta, r1.w, C1);
-                    C2 = __fmaf_rn(ta, s_rec[j].r2.x, C2);
-                    T = T * (1.0f - alpha);
-                    if (T < 1e-4f) { done = true; cnt = rbase + j + 1; }
-                  }
+            if (!done) {
+              const float4 r0 = s_rec[j].r0;
+              const float4 r1 = s_rec[j].r1;
+              const float dx = px - r0.x, dy = py - r0.y;
+              const float ee = pairExponent(r0, r1.x, dx, dy);
+              if (ee <= E_CUT) {
+                const float araw = r1.y * gexp(-ee);
+                const float alpha = fminf(0.99f, araw);
+                if (alpha >= A_MIN) {
+                  contrib = true;
+                  if (STORED) a.tStore[(size_t)(base + j) * RTHREADS + tid] = T;
+                  const float ta = T * alpha;
+                  C0 = __fmaf_rn(ta, r1.z, C0);
+                  C1 = __fmaf_rn(ta, r1.w, C1);
+                  C2 = __fmaf_rn(ta, s_rec[j].r2.x, C2);
+                  T = T * (1.0f - alpha);
+                  if (T < 1e-4f) { done = true; cnt = rbase + j + 1; }
                 }
               }
-              if (MASKS && __ballot_sync(FULL, contrib)) bits |= 1u << (j & 31);
             }
-            const bool allDone = __all_sync(FULL, done);
-            if (MASKS && ((j & 31) == 31 || j + 1 == nb || allDone)) {
-              const uint32_t w = (rbase + j) >> 5;
-              if (lane == 0 && w < MASKW) wmask[w] = bits;
-              bits = 0;
+            if (MASKS) bits |= (__ballot_sync(FULL, contrib) != 0u ? 1u : 0u) << (j & 31);
+            if ((j & 31) == 31 || j + 1 == nb) {  // word boundary: store bits, leave when all saturated
+              if (MASKS) {
+                const uint32_t w = (rbase + j) >> 5;
+                if (lane == 0 && w < MASKW) wmask[w] = bits;
+                bits = 0;
+              }
+              if (__all_sync(FULL, done)) break;
             }
-            if (allDone) break;
           }
         }
         __syncthreads();
@@ -221,7 +224,7 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
       __syncthreads();
       if (tid < 5) {
         uint32_t sum = 0;
-        for (int w = 0; w < 8; ++w) sum += s_redu[w][tid];
+        for (int w = 0; w < NW; ++w) sum += s_redu[w][tid];
         if (sum) {
           if (tid < 3) atomicAdd(&a.stats[tid], sum);
           else atomicAdd(&a.gradCam[c.camIdx * 8u + 3u + (uint32_t)tid], (int32_t)sum);
@@ -229,7 +232,7 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
       }
       uint32_t endMax = 0;
 #pragma unroll
-      for (int w = 0; w < 8; ++w) endMax = max(endMax, s_endmax[w]);
+      for (int w = 0; w < NW; ++w) endMax = max(endMax, s_endmax[w]);
       // ---- backward (shaders.js:632-700) ----
       float S0 = c.bg[0] * T, S1 = c.bg[1] * T, S2 = c.bg[2] * T;
       float Ta = T;
@@ -331,46 +334,56 @@ __global__ void __launch_bounds__(RTHREADS) k_raster(RasterArgs a) {
   }
 }
 
-template <int BATCH, bool FWD, bool BWD, bool STORED>
+template <int TILE, int BATCH, bool FWD, bool BWD, bool STORED>
 static void launch_one(const RasterArgs& a, unsigned grid, cudaStream_t s) {
-  k_raster<BATCH, FWD, BWD, STORED><<<grid, RTHREADS, 0, s>>>(a);
+  k_raster<TILE, BATCH, FWD, BWD, STORED><<<grid, TILE * TILE, 0, s>>>(a);
 }
 
-template <int BATCH>
-static void launch_batch(const RasterArgs& a, int mode, bool stored, unsigned grid, cudaStream_t s) {
+template <int TILE, int BATCH>
+static void launch_mode(const RasterArgs& a, int mode, bool stored, unsigned grid, cudaStream_t s) {
   // mode: 1 = forward, 2 = backward from saved state, 3 = fused train tile
-  if (mode == 1) {
-    if (stored) launch_one<BATCH, true, false, true>(a, grid, s);
-    else launch_one<BATCH, true, false, false>(a, grid, s);
-  } else if (mode == 2) {
-    if (stored) launch_one<BATCH, false, true, true>(a, grid, s);
-    else launch_one<BATCH, false, true, false>(a, grid, s);
+  if (mode == 1) launch_one<TILE, BATCH, true, false, false>(a, grid, s);
+  else if (mode == 2) {
+    if (stored) launch_one<TILE, BATCH, false, true, true>(a, grid, s);
+    else launch_one<TILE, BATCH, false, true, false>(a, grid, s);
   } else {
-    if (stored) launch_one<BATCH, true, true, true>(a, grid, s);
-    else launch_one<BATCH, true, true, false>(a, grid, s);
+    if (stored) launch_one<TILE, BATCH, true, true, true>(a, grid, s);
+    else launch_one<TILE, BATCH, true, true, false>(a, grid, s);
   }
 }
 
-void launch_raster(const RasterArgs& a, int mode, bool stored, int batchDepth, unsigned grid, cudaStream_t s) {
+template <int TILE>
+static void launch_tile(const RasterArgs& a, int mode, bool stored, int batchDepth, unsigned grid, cudaStream_t s) {
+  switch (batchDepth) {
+    case 64: launch_mode<TILE, 64>(a, mode, stored, grid, s); break;
+    case 128: launch_mode<TILE, 128>(a, mode, stored, grid, s); break;
+    default: launch_mode<TILE, 256>(a, mode, stored, grid, s); break;
+  }
+}
+
+void launch_raster(const RasterArgs& a, int mode, bool stored, int tile, int batchDepth, unsigned grid,
+                   cudaStream_t s) {
   if (grid == 0) return;
+  if (tile == 8) launch_tile<8>(a, mode, stored, batchDepth, grid, s);
+  else if (tile == 32) launch_tile<32>(a, mode, stored, batchDepth, grid, s);
+  else launch_tile<16>(a, mode, stored, batchDepth, grid, s);
+}
+
+template <int TILE>
+static const void* kernel_of(int batchDepth, int mode) {
+  const bool fwdOnly = mode == 1;
   switch (batchDepth) {
-    case 32: launch_batch<32>(a, mode, stored, grid, s); break;
-    case 64: launch_batch<64>(a, mode, stored, grid, s); break;
-    case 128: launch_batch<128>(a, mode, stored, grid, s); break;
-    default: launch_batch<256>(a, mode, stored, grid, s); break;
+    case 64: return fwdOnly ? (const void*)k_raster<TILE, 64, true, false, false> : (const void*)k_raster<TILE, 64, true, true, false>;
+    case 128: return fwdOnly ? (const void*)k_raster<TILE, 128, true, false, false> : (const void*)k_raster<TILE, 128, true, true, false>;
+    default: return fwdOnly ? (const void*)k_raster<TILE, 256, true, false, false> : (const void*)k_raster<TILE, 256, true, true, false>;
   }
 }
 
-int raster_blocks_per_sm(int batchDepth, int mode) {
+int raster_blocks_per_sm(int tile, int batchDepth, int mode) {
+  const void* f = tile == 8 ? kernel_of<8>(batchDepth, mode) : tile == 32 ? kernel_of<32>(batchDepth, mode)
+                                                                          : kernel_of<16>(batchDepth, mode);
   int perSm = 0;
-  const void* f;
-  switch (batchDepth) {
-    case 32: f = mode == 1 ? (const void*)k_raster<32, true, false, false> : (const void*)k_raster<32, true, true, false>; break;
-    case 64: f = mode == 1 ? (const void*)k_raster<64, true, false, false> : (const void*)k_raster<64, true, true, false>; break;
-    case 128: f = mode == 1 ? (const void*)k_raster<128, true, false, false> : (const void*)k_raster<128, true, true, false>; break;
-    default: f = mode == 1 ? (const void*)k_raster<256, true, false, false> : (const void*)k_raster<256, true, true, false>; break;
-  }
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, f, RTHREADS, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, f, tile * tile, 0);
   return perSm < 1 ? 1 : perSm;
 }
 

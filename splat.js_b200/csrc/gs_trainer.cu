@@ -43,6 +43,8 @@ struct Shape {
   int adam;
   int grads;      // write gradF/shGrad readout
   int variant;
+  int tile;       // raster tile edge
+  int depth;      // splat-batch depth
   bool operator<(const Shape& o) const { return std::memcmp(this, &o, sizeof(Shape)) < 0; }
 };
 
@@ -121,7 +123,8 @@ struct gs_trainer {
 
   std::map<Shape, cudaGraphExec_t> graphs;
   int histGrid = 0, sweepGrid = 0;
-  int rasterPerSm[2] = {1, 1};
+  int tile = 16;                 // current raster tile edge (8, 16 or 32)
+  int rasterPerSm[3][3][2] = {};  // occupancy per (tile, batch depth, forward-only / train)
 
   // ---- measurement ----
   cudaStream_t ownStream = nullptr;
@@ -185,8 +188,8 @@ static DevCam make_cam(const gs_trainer* h, const gs_camera& c, int train, uint3
   d.bias = (float)c.b;
   d.activeSh = activeSh;
   d.W = c.w; d.H = c.h;
-  d.tilesX = (int)ceil_div((uint32_t)c.w, 16);
-  d.tilesY = (int)ceil_div((uint32_t)c.h, 16);
+  d.tilesX = (int)ceil_div((uint32_t)c.w, (uint32_t)h->tile);
+  d.tilesY = (int)ceil_div((uint32_t)c.h, (uint32_t)h->tile);
   d.offset = offset;
   d.camIdx = camIdx;
   d.ncams = h->ncams;
@@ -234,9 +237,9 @@ int gs_create(const gs_options* opts, gs_trainer** out) {
   gs_options o;
   if (opts) o = *opts; else gs_default_options(&o);
   if (o.shDeg < 0 || o.shDeg > 3) { g_createError = "shDeg must be 0..3"; return GS_E_INVALID; }
-  if (o.tile != 16) { g_createError = "tile: only 16 is implemented"; return GS_E_INVALID; }
-  if (o.batchDepth != 32 && o.batchDepth != 64 && o.batchDepth != 128 && o.batchDepth != 256) {
-    g_createError = "batchDepth must be 32, 64, 128 or 256";
+  if (o.tile != 8 && o.tile != 16 && o.tile != 32) { g_createError = "tile must be 8, 16 or 32"; return GS_E_INVALID; }
+  if (o.batchDepth != 64 && o.batchDepth != 128 && o.batchDepth != 256) {
+    g_createError = "batchDepth must be 64, 128 or 256";
     return GS_E_INVALID;
   }
   if (o.maxBatch < 1 || o.maxBatch > MAXB) { g_createError = "maxBatch must be 1..16"; return GS_E_INVALID; }
@@ -261,8 +264,11 @@ int gs_create(const gs_options* opts, gs_trainer** out) {
   h->horizon = o.maxIters ? o.maxIters : 60000u;
   h->histGrid = h->sms * 4;
   h->sweepGrid = onesweep_grid(h->device);
-  h->rasterPerSm[0] = raster_blocks_per_sm(o.batchDepth, 1);
-  h->rasterPerSm[1] = raster_blocks_per_sm(o.batchDepth, 3);
+  h->tile = o.tile;
+  for (int ti = 0; ti < 3; ++ti)
+    for (int di = 0; di < 3; ++di)
+      for (int m = 0; m < 2; ++m)
+        h->rasterPerSm[ti][di][m] = raster_blocks_per_sm(8 << ti, 64 << di, m == 0 ? 1 : 3);
   *out = h;
   return GS_OK;
 }
@@ -335,13 +341,15 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   }
   // view limits
   h->maxPix = maxViewW * maxViewH;
-  h->maxTiles = ceil_div(maxViewW, 16) * ceil_div(maxViewH, 16);
-  h->maxGrid = (ceil_div(maxViewW, 16) + 1) * (ceil_div(maxViewH, 16) + 1);
+  // tile-indexed buffers are sized for the smallest tile (8) so the tile
+  // size can change after setup (gs_autotune)
+  h->maxTiles = ceil_div(maxViewW, 8) * ceil_div(maxViewH, 8);
+  h->maxGrid = (ceil_div(maxViewW, 8) + 1) * (ceil_div(maxViewH, 8) + 1);
   for (uint32_t c = 0; c < ncams; ++c) {
     const uint32_t w = (uint32_t)h->cams[c].w, hh = (uint32_t)h->cams[c].h;
     h->maxPix = std::max(h->maxPix, w * hh);
-    h->maxTiles = std::max(h->maxTiles, ceil_div(w, 16) * ceil_div(hh, 16));
-    h->maxGrid = std::max(h->maxGrid, (ceil_div(w, 16) + 1) * (ceil_div(hh, 16) + 1));
+    h->maxTiles = std::max(h->maxTiles, ceil_div(w, 8) * ceil_div(hh, 8));
+    h->maxGrid = std::max(h->maxGrid, (ceil_div(w, 8) + 1) * (ceil_div(hh, 8) + 1));
   }
   const uint32_t B = (uint32_t)o.maxBatch;
   const size_t cap = h->cap, shn = (size_t)h->cap * 3 * h->K;
@@ -513,7 +521,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   const int V = sh.V;
   uint32_t totalTiles = 0, gridCells = 0;
   for (int v = 0; v < V; ++v) {
-    const uint32_t tx = ceil_div((uint32_t)sh.w[v], 16), ty = ceil_div((uint32_t)sh.h[v], 16);
+    const uint32_t tx = ceil_div((uint32_t)sh.w[v], (uint32_t)sh.tile), ty = ceil_div((uint32_t)sh.h[v], (uint32_t)sh.tile);
     totalTiles += tx * ty;
     gridCells += (tx + 1) * (ty + 1);
   }
@@ -544,7 +552,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   pa.eCut = h->o.eCut;
   pa.aMin = h->o.aMin;
   pa.radClamp = h->o.radClamp;
-  pa.tile = 16;
+  pa.tile = sh.tile;
   pa.recs = h->recs;
   pa.depth = h->depth;
   pa.rect = h->rect;
@@ -636,10 +644,12 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   rr.tStore = h->tStore;
   unsigned grid = totalTiles;
   if (persistent) {
-    const unsigned full = (unsigned)(h->sms * (sh.mode == 1 ? h->rasterPerSm[0] : h->rasterPerSm[1]));
+    const int ti = sh.tile == 8 ? 0 : sh.tile == 16 ? 1 : 2;
+    const int di = sh.depth == 64 ? 0 : sh.depth == 128 ? 1 : 2;
+    const unsigned full = (unsigned)(h->sms * h->rasterPerSm[ti][di][sh.mode == 1 ? 0 : 1]);
     grid = std::min(grid, full);
   }
-  launch_raster(rr, sh.mode, sh.variant == 1, h->o.batchDepth, grid, s);
+  launch_raster(rr, sh.mode, sh.variant == 1, sh.tile, sh.depth, grid, s);
   if (h->profiling) cudaEventRecord(ph[3], s);
 
   if (sh.chain) {
@@ -691,7 +701,7 @@ static int ensure_tstore(gs_trainer* h, const Shape& sh) {
   uint32_t E = 0;
   GS_CK(cudaMemcpyAsync(&E, h->small + 2057, 4, cudaMemcpyDeviceToHost, h->stream));
   GS_CK(cudaStreamSynchronize(h->stream));
-  const size_t need = (size_t)E * 256 + 1;
+  const size_t need = (size_t)E * sh.tile * sh.tile + 1;  // T per (entry, pixel of its tile)
   if (need > h->tStoreCap) {
     if (h->tStore) cudaFree(h->tStore);
     h->tStore = nullptr;
@@ -771,6 +781,8 @@ static Shape make_shape(gs_trainer* h, const DevCam* views, int V, int mode, int
   sh.adam = adam;
   sh.grads = grads;
   sh.variant = h->o.backwardVariant;
+  sh.tile = h->tile;
+  sh.depth = h->o.batchDepth;
   return sh;
 }
 
@@ -873,7 +885,7 @@ int gs_render(gs_trainer* h, const gs_camera* cam, int32_t trainMode, uint32_t o
   if (!h->ready) return fail(h, GS_E_INVALID, "setup() first");
   if ((uint64_t)cam->w * cam->h > h->maxPix || cam->w <= 0 || cam->h <= 0)
     return fail(h, GS_E_LIMIT, "renderView: view larger than setup's maxViewW x maxViewH");
-  if (ceil_div((uint32_t)cam->w, 16) * ceil_div((uint32_t)cam->h, 16) > h->maxTiles)
+  if (ceil_div((uint32_t)cam->w, (uint32_t)h->tile) * ceil_div((uint32_t)cam->h, (uint32_t)h->tile) > h->maxTiles)
     return fail(h, GS_E_LIMIT, "renderView: view has more tiles than setup's maximum");
   if (trainMode && (uint64_t)offset + (uint64_t)cam->w * cam->h > h->totalPix)
     return fail(h, GS_E_LIMIT, "renderView: trainMode target offset + view size exceeds the training targets");
@@ -1014,6 +1026,73 @@ int gs_debug_gradp(gs_trainer* h, uint32_t view, int32_t* gradP10, int32_t clear
   if (gradP10)
     for (size_t i = 0; i < h->n; ++i)
       for (int k = 0; k < 10; ++k) gradP10[i * 10 + k] = tmp[i * GP_STRIDE + k];
+  return GS_OK;
+}
+
+// Autotuner: times the training pass (raster + chain, parameters untouched)
+// on views ci[0..nviews) for every tile edge {8, 16, 32} x splat-batch depth
+// {64, 128, 256} and keeps the fastest.  Loss statistics and camera
+// gradients accumulated meanwhile are restored.
+int gs_autotune(gs_trainer* h, const uint32_t* ci, uint32_t nv, int32_t reps, int32_t* bestTile, int32_t* bestDepth,
+                float* msOut) {
+  if (!h) return GS_E_INVALID;
+  int rc = check_views(h, ci, nv);
+  if (rc) return rc;
+  if (reps < 1) reps = 1;
+  cudaSetDevice(h->device);
+  cudaStream_t s = h->stream;
+  uint32_t st[4];
+  std::vector<int32_t> cg((size_t)(h->ncams + 1) * 8);
+  GS_CK(cudaMemcpyAsync(st, h->stats, 16, cudaMemcpyDeviceToHost, s));
+  GS_CK(cudaMemcpyAsync(cg.data(), h->gradCam, cg.size() * 4, cudaMemcpyDeviceToHost, s));
+  GS_CK(cudaStreamSynchronize(s));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int tiles[3] = {8, 16, 32}, depths[3] = {64, 128, 256};
+  float best = 3.0e38f;
+  int bt = h->tile, bd = h->o.batchDepth;
+  for (int ti = 0; ti < 3 && rc == GS_OK; ++ti)
+    for (int di = 0; di < 3 && rc == GS_OK; ++di) {
+      h->tile = tiles[ti];
+      h->o.batchDepth = depths[di];
+      DevCam views[MAXB];
+      for (uint32_t k = 0; k < nv; ++k)
+        views[k] = make_cam(h, h->cams[ci[k]], 1, h->camOffset[ci[k]], ci[k], h->camActiveSh[ci[k]]);
+      upload_params(h, views, (int)nv, make_hp(h));
+      const Shape sh = make_shape(h, views, (int)nv, 3, 1, 0, 0);
+      rc = run_shape(h, sh);  // warm-up (and graph capture)
+      if (rc) break;
+      cudaEventRecord(e0, s);
+      for (int r = 0; r < reps && rc == GS_OK; ++r) rc = run_shape(h, sh);
+      cudaEventRecord(e1, s);
+      cudaEventSynchronize(e1);
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      ms /= (float)reps;
+      if (msOut) msOut[ti * 3 + di] = ms;
+      if (ms < best) { best = ms; bt = tiles[ti]; bd = depths[di]; }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->tile = bt;
+  h->o.batchDepth = bd;
+  cudaMemcpyAsync(h->stats, st, 16, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(h->gradCam, cg.data(), cg.size() * 4, cudaMemcpyHostToDevice, s);
+  GS_CK(cudaStreamSynchronize(s));
+  if (rc) return rc;
+  if (bestTile) *bestTile = bt;
+  if (bestDepth) *bestDepth = bd;
+  return check_status(h);
+}
+
+int gs_set_raster_config(gs_trainer* h, int32_t tile, int32_t batchDepth) {
+  if (!h) return GS_E_INVALID;
+  if (tile != 8 && tile != 16 && tile != 32) return fail(h, GS_E_INVALID, "tile must be 8, 16 or 32");
+  if (batchDepth != 64 && batchDepth != 128 && batchDepth != 256)
+    return fail(h, GS_E_INVALID, "batchDepth must be 64, 128 or 256");
+  h->tile = tile;
+  h->o.batchDepth = batchDepth;
   return GS_OK;
 }
 

@@ -94,6 +94,8 @@ def lib():
         "gs_profile": (C.c_int, [H, C.c_int32]),
         "gs_profile_read": (C.c_int, [H, P(C.c_double), u32p]),
         "gs_probe_fp32_peak": (C.c_int, [C.c_int32, P(C.c_double)]),
+        "gs_autotune": (C.c_int, [H, u32p, C.c_uint32, C.c_int32, i32p, i32p, f32p]),
+        "gs_set_raster_config": (C.c_int, [H, C.c_int32, C.c_int32]),
         "gs_raster_pass": (C.c_int, [H, u32p, C.c_uint32, C.c_int32]),
         "gs_debug_records": (C.c_int, [H, C.c_uint32, f32p, u32p]),
         "gs_debug_binning": (C.c_int, [H, C.c_uint32, u32p, u32p, u32p, C.c_uint64, u64p]),

@@ -365,6 +365,23 @@ class GSTrainer:
         return {"moved": int(out.moved), "grown": int(out.grown), "n": int(out.n), "maxTile": int(out.maxTile),
                 "overflow": int(out.overflow)}
 
+    # ---- raster configuration ----
+    def autotune(self, cams=None, reps=3):
+        """Pick tile size {8,16,32} x splat-batch depth {64,128,256} by timing
+        the training pass on `cams` (default: the first few cameras).
+        Returns (tile, depth, {(tile, depth): ms})."""
+        if cams is None:
+            cams = list(range(min(len(self.camMeta), int(self._o.maxBatch))))
+        arr = (C.c_uint32 * len(cams))(*[int(c) for c in cams])
+        bt, bd = C.c_int32(), C.c_int32()
+        ms = (C.c_float * 9)()
+        N.check(N.lib().gs_autotune(self._h, arr, len(cams), int(reps), C.byref(bt), C.byref(bd), ms), self._h)
+        table = {(8 << i, 64 << j): ms[i * 3 + j] for i in range(3) for j in range(3)}
+        return bt.value, bd.value, table
+
+    def setRasterConfig(self, tile, depth):
+        N.check(N.lib().gs_set_raster_config(self._h, int(tile), int(depth)), self._h)
+
     # ---- gradient check support (gradcheck.js:266-356) ----
     def gradPass(self, ci=0):
         """encodeRaster + chain without Adam; returns (gradF, shGrad, stats)."""

@@ -41,7 +41,7 @@ def make(params, sh, cams, rgbs, opts, radius=1.5, maxW=None, maxH=None):
 def oracle_opts(opts):
     return O.opts(eCut=opts.get("eCut", 4.5), aMin=opts.get("aMin", 0.0039), radClamp=opts.get("radClamp", 1.0),
                   anisoReg=opts.get("anisoReg", 0.005), shDeg=opts.get("shDeg", 2),
-                  entriesCap=opts.get("entriesCap", 12_000_000))
+                  entriesCap=opts.get("entriesCap", 12_000_000), tile=opts.get("tile", 16))
 
 
 def gpu_raster(t, cis, mode=3):
@@ -51,14 +51,14 @@ def gpu_raster(t, cis, mode=3):
     N.check(N.lib().gs_raster_pass(t._h, arr, len(cis), mode), t._h)
 
 
-def gpu_view(t, view, meta, n):
+def gpu_view(t, view, meta, n, tile=16):
     import ctypes as C
     from splat_b200 import native as N
     L = N.lib()
     rec = np.zeros(n * 12, np.float32)
     rect = np.zeros(n * 2, np.uint32)
     N.check(L.gs_debug_records(t._h, view, N.ptr(rec), N.ptr(rect, C.c_uint32)), t._h)
-    nt = ((meta["w"] + 15) // 16) * ((meta["h"] + 15) // 16)
+    nt = ((meta["w"] + tile - 1) // tile) * ((meta["h"] + tile - 1) // tile)
     cnt = np.zeros(nt, np.uint32)
     rg = np.zeros(nt * 2, np.uint32)
     nE = C.c_uint64()
@@ -93,7 +93,7 @@ def assert_bits(a, b, what):
 
 
 def check_view_against_oracle(t, o, ocam, params, sh, targets, n, view=0):
-    g = gpu_view(t, view, dict(w=ocam.w, h=ocam.h), n)
+    g = gpu_view(t, view, dict(w=ocam.w, h=ocam.h), n, tile=o.tile)
     proj = O.project(o, ocam, params, sh if o.shDeg else None, n)
     rec, rect = O.records(o, ocam, proj, n)
     vis = rect[0::2] != 0xFFFFFFFF
@@ -349,3 +349,39 @@ def test_refine_matches_oracle():
     # and training continues on the grown model
     t.stepBatch([0])
     assert t.readGaussians()["n"] == n2
+
+
+@pytest.mark.parametrize("tile", [8, 32])
+def test_other_tile_sizes_bitexact(tile):
+    """Tile 8 and 32 have no reference counterpart: their per-tile entry lists
+    match the oracle binned at that tile size, and images, transmittance and
+    gradients equal the tile-16 (reference) results bit for bit."""
+    params, sh, cams, rgbs = config0(n=20000, seed=4)
+    n = len(params) // 16
+    opts = dict(shDeg=2, tile=tile)
+    t, targets, metas = make(params, sh, cams, rgbs, opts, radius=1.0)
+    gpu_raster(t, [0], 3)
+    check_view_against_oracle(t, oracle_opts(opts), oracle_cam(metas[0], 0, 1, 2), params, sh, targets, n)
+    t16, _, _ = make(params, sh, cams, rgbs, dict(shDeg=2), radius=1.0)
+    g, sg, st = t.gradPass(0)
+    g16, sg16, st16 = t16.gradPass(0)
+    assert_bits(g, g16, f"gradF tile {tile} vs 16")
+    assert_bits(sg, sg16, f"shGrad tile {tile} vs 16")
+    assert_bits(st, st16, f"stats tile {tile} vs 16")
+    img = t.renderView(metas[0])
+    img16 = t16.renderView(metas[0])
+    assert_bits(img, img16, f"image tile {tile} vs 16")
+
+
+def test_autotune_picks_a_config_and_keeps_results():
+    params, sh, cams, rgbs = config0(n=20000, seed=6)
+    n = len(params) // 16
+    t, targets, metas = make(params, sh, cams, rgbs, dict(shDeg=2), radius=1.0)
+    g0, s0, st0 = t.gradPass(0)
+    tile, depth, table = t.autotune([0], reps=1)
+    assert tile in (8, 16, 32) and depth in (64, 128, 256)
+    assert all(v > 0 for v in table.values()), table
+    assert min(table.values()) == table[(tile, depth)]
+    g1, s1, st1 = t.gradPass(0)
+    assert_bits(g1, g0, "gradF after autotune")
+    assert_bits(st1, st0, "stats after autotune")
