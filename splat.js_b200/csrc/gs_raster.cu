@@ -124,28 +124,29 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
           const uint32_t rbase = base - s;
           uint32_t bits = 0;
           for (uint32_t j = 0; j < nb; ++j) {
-            bool contrib = false;
-            if (!done) {
-              const float4 r0 = s_rec[j].r0;
-              const float4 r1 = s_rec[j].r1;
-              const float dx = px - r0.x, dy = py - r0.y;
-              const float ee = pairExponent(r0, r1.x, dx, dy);
-              if (ee <= E_CUT) {
-                const float araw = r1.y * gexp(-ee);
-                const float alpha = fminf(0.99f, araw);
-                if (alpha >= A_MIN) {
-                  contrib = true;
-                  if (STORED) a.tStore[(size_t)(base + j) * RTHREADS + tid] = T;
-                  const float ta = T * alpha;
-                  C0 = __fmaf_rn(ta, r1.z, C0);
-                  C1 = __fmaf_rn(ta, r1.w, C1);
-                  C2 = __fmaf_rn(ta, s_rec[j].r2.x, C2);
-                  T = T * (1.0f - alpha);
-                  if (T < 1e-4f) { done = true; cnt = rbase + j + 1; }
-                }
+            const float4 r0 = s_rec[j].r0;
+            const float4 r1 = s_rec[j].r1;
+            const float dx = px - r0.x, dy = py - r0.y;
+            const float ee = pairExponent(r0, r1.x, dx, dy);
+            const bool c1 = !done && ee <= E_CUT;
+            // warp-uniform branch; the body runs predicated per lane (lanes
+            // outside the cutoff see a clamped exponent and are masked off)
+            if (__any_sync(FULL, c1)) {
+              const float araw = r1.y * gexp(-fminf(ee, 80.0f));
+              const float alpha = fminf(0.99f, araw);
+              const bool c2 = c1 && alpha >= A_MIN;
+              if (STORED && c2) a.tStore[(size_t)(base + j) * RTHREADS + tid] = T;
+              const float ta = T * alpha;
+              const float cb = s_rec[j].r2.x;
+              if (c2) {
+                C0 = __fmaf_rn(ta, r1.z, C0);
+                C1 = __fmaf_rn(ta, r1.w, C1);
+                C2 = __fmaf_rn(ta, cb, C2);
+                T = T * (1.0f - alpha);
+                if (T < 1e-4f) { done = true; cnt = rbase + j + 1; }
               }
+              if (MASKS) bits |= (__ballot_sync(FULL, c2) != 0u ? 1u : 0u) << (j & 31);
             }
-            if (MASKS) bits |= (__ballot_sync(FULL, contrib) != 0u ? 1u : 0u) << (j & 31);
             if ((j & 31) == 31 || j + 1 == nb) {  // word boundary: store bits, leave when all saturated
               if (MASKS) {
                 const uint32_t w = (rbase + j) >> 5;
@@ -262,60 +263,57 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
             continue;
           }
           jn = (int32_t)j - 1;
+          // Straight-line body, predicated per lane: lanes that do not
+          // composite this entry (past their end, outside a cutoff) compute
+          // on a clamped exponent and have their contribution zeroed through
+          // galpha and aT, and keep S and Ta.  Composing lanes perform
+          // exactly the canonical sequence.
           const RenderRec& rr = s_rec[j - lo];
-          int32_t q[10];
-#pragma unroll
-          for (int k = 0; k < 10; ++k) q[k] = 0;
-          bool contrib = false;
-          if (j < myEnd) {
-            const float4 r0 = rr.r0;
-            const float4 r1 = rr.r1;
-            const float dx = px - r0.x, dy = py - r0.y;
-            const float ee = pairExponent(r0, r1.x, dx, dy);
-            if (ee <= E_CUT) {
-              const float G = gexp(-ee);
-              const float araw = r1.y * G;
-              const float alpha = fminf(0.99f, araw);
-              if (alpha >= A_MIN) {
-                contrib = true;
-                const float4 r2 = rr.r2;
-                const float inv = __frcp_rn(1.0f - alpha);
-                const float Tb = STORED ? a.tStore[(size_t)(s + j) * RTHREADS + tid] : Ta * inv;
-                const float aT = alpha * Tb;
-                const float g0 = __fmaf_rn(r1.z, Tb, -(S0 * inv));
-                const float g1 = __fmaf_rn(r1.w, Tb, -(S1 * inv));
-                const float g2 = __fmaf_rn(r2.x, Tb, -(S2 * inv));
-                float galpha = __fmaf_rn(gC2, g2, __fmaf_rn(gC1, g1, gC0 * g0));
-                if (araw > 0.99f) galpha = 0.0f;
-                const float gal16 = galpha * FIXED;
-                const float ga16 = gal16 * araw;
-                q[0] = fix_scaled(ga16 * __fmaf_rn(r0.z, dx, r0.w * dy));
-                q[1] = fix_scaled(ga16 * __fmaf_rn(r0.w, dx, r1.x * dy));
-                const float gq16 = ga16 * (-0.5f * r2.z);
-                const float gqx16 = gq16 * dx;
-                q[2] = fix_scaled(gqx16 * dx);
-                q[3] = fix_scaled((gqx16 * dy) * 2.0f);
-                q[4] = fix_scaled((gq16 * dy) * dy);
-                q[5] = fix_scaled((gal16 * r2.y) * G);
-                q[6] = fix_scaled(ga16 * (1.0f - r2.y));
-                q[7] = fix_scaled(g16_0 * aT);
-                q[8] = fix_scaled(g16_1 * aT);
-                q[9] = fix_scaled(g16_2 * aT);
-                S0 = __fmaf_rn(r1.z, aT, S0);
-                S1 = __fmaf_rn(r1.w, aT, S1);
-                S2 = __fmaf_rn(r2.x, aT, S2);
-                Ta = Tb;
-              }
-            }
-          }
-          if (__any_sync(FULL, contrib)) {
+          const float4 r0 = rr.r0;
+          const float4 r1 = rr.r1;
+          const float4 r2 = rr.r2;
+          const float dx = px - r0.x, dy = py - r0.y;
+          const float ee = pairExponent(r0, r1.x, dx, dy);
+          const float G = gexp(-fminf(ee, 80.0f));
+          const float araw = r1.y * G;
+          const float alpha = fminf(0.99f, araw);
+          const bool c2 = j < myEnd && ee <= E_CUT && alpha >= A_MIN;
+          if (__any_sync(FULL, c2)) {
+            const float inv = __frcp_rn(1.0f - alpha);
+            const float Tb = STORED ? (c2 ? a.tStore[(size_t)(s + j) * RTHREADS + tid] : 0.0f) : Ta * inv;
+            const float aT = c2 ? alpha * Tb : 0.0f;
+            const float g0 = __fmaf_rn(r1.z, Tb, -(S0 * inv));
+            const float g1 = __fmaf_rn(r1.w, Tb, -(S1 * inv));
+            const float g2 = __fmaf_rn(r2.x, Tb, -(S2 * inv));
+            float galpha = __fmaf_rn(gC2, g2, __fmaf_rn(gC1, g1, gC0 * g0));
+            if (araw > 0.99f) galpha = 0.0f;
+            const float gal16 = c2 ? galpha * FIXED : 0.0f;
+            const float ga16 = gal16 * araw;
+            const float gq16 = ga16 * (-0.5f * r2.z);
+            const float gqx16 = gq16 * dx;
             uint32_t r[10];
+            r[0] = __reduce_add_sync(FULL, (uint32_t)fix_scaled(ga16 * __fmaf_rn(r0.z, dx, r0.w * dy)));
+            r[1] = __reduce_add_sync(FULL, (uint32_t)fix_scaled(ga16 * __fmaf_rn(r0.w, dx, r1.x * dy)));
+            r[2] = __reduce_add_sync(FULL, (uint32_t)fix_scaled(gqx16 * dx));
+            r[3] = __reduce_add_sync(FULL, (uint32_t)fix_scaled((gqx16 * dy) * 2.0f));
+            r[4] = __reduce_add_sync(FULL, (uint32_t)fix_scaled((gq16 * dy) * dy));
+            r[5] = __reduce_add_sync(FULL, (uint32_t)fix_scaled((gal16 * r2.y) * G));
+            r[6] = __reduce_add_sync(FULL, (uint32_t)fix_scaled(ga16 * (1.0f - r2.y)));
+            r[7] = __reduce_add_sync(FULL, (uint32_t)fix_scaled(g16_0 * aT));
+            r[8] = __reduce_add_sync(FULL, (uint32_t)fix_scaled(g16_1 * aT));
+            r[9] = __reduce_add_sync(FULL, (uint32_t)fix_scaled(g16_2 * aT));
+            if (c2) {
+              S0 = __fmaf_rn(r1.z, aT, S0);
+              S1 = __fmaf_rn(r1.w, aT, S1);
+              S2 = __fmaf_rn(r2.x, aT, S2);
+              Ta = Tb;
+            }
+            if (lane == 0) {
+              int32_t* acc = s_acc + (j - lo) * 10;
 #pragma unroll
-            for (int k = 0; k < 10; ++k) r[k] = __reduce_add_sync(FULL, (uint32_t)q[k]);
-            uint32_t mine = r[0];
-#pragma unroll
-            for (int k = 1; k < 10; ++k) mine = lane == k ? r[k] : mine;
-            if (lane < 10 && mine) atomicAdd(&s_acc[(j - lo) * 10 + lane], (int32_t)mine);
+              for (int k = 0; k < 10; ++k)
+                if (r[k]) atomicAdd(&acc[k], (int32_t)r[k]);
+            }
           }
         }
         __syncthreads();

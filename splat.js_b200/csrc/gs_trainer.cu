@@ -237,6 +237,8 @@ int gs_create(const gs_options* opts, gs_trainer** out) {
   gs_options o;
   if (opts) o = *opts; else gs_default_options(&o);
   if (o.shDeg < 0 || o.shDeg > 3) { g_createError = "shDeg must be 0..3"; return GS_E_INVALID; }
+  // exp(-e) is evaluated for e <= eCut; the canonical exp is defined on |x| <= 87
+  if (!(o.eCut > 0.0f && o.eCut <= 80.0f)) { g_createError = "eCut must be in (0, 80]"; return GS_E_INVALID; }
   if (o.tile != 8 && o.tile != 16 && o.tile != 32) { g_createError = "tile must be 8, 16 or 32"; return GS_E_INVALID; }
   if (o.batchDepth != 64 && o.batchDepth != 128 && o.batchDepth != 256) {
     g_createError = "batchDepth must be 64, 128 or 256";
