@@ -205,7 +205,7 @@ GS_API int gs_set_raster_config(gs_trainer* h, int32_t tile, int32_t batchDepth)
  * ci[0..nviews); mode 1 = forward only, 3 = forward + loss + backward. */
 GS_API int gs_raster_pass(gs_trainer* h, const uint32_t* ci, uint32_t nviews, int32_t mode);
 /* Per-splat raster record of view slot `view`: rec n*12 f32
- * (mx, my, cA, cB, cC, opa*comp, r, g, b, opa, 1/(1+lambda_max), depth),
+ * (mx, my, cA/2, cB, cC/2, opa*comp, r, g, b, opa, 1/(1+lambda_max), cull radius),
  * rect n*2 u32 (x0 | y0<<16, x1 | y1<<16; 0xFFFFFFFF = culled). */
 GS_API int gs_debug_records(gs_trainer* h, uint32_t view, float* rec12, uint32_t* rect2);
 /* Binning of view slot `view`: tileCnt[tiles], ranges[2*tiles] (global entry

@@ -525,7 +525,7 @@ struct PixelState {
 // (shaders.js:544-700).  Canonical FP32 arithmetic of the per-pair loop --
 // the CUDA rasteriser evaluates exactly these operations:
 //   dx = px - mx; dy = py - my
-//   e  = max(fma(0.5, fma(cA*dx, dx, (cC*dy)*dy), (cB*dx)*dy), 0)
+//   e  = max(fma(fma(cA/2, dx, cB*dy), dx, ((cC/2)*dy)*dy), 0)
 //   G  = exp(-e); araw = w*G (w = opa*comp); alpha = min(0.99, araw)
 //   fwd: ta = T*alpha; C = fma(ta, c, C); T = T*(1 - alpha)
 //   bwd: inv = 1/(1 - alpha); Tb = Ta*inv; aT = alpha*Tb; gcv = gC*aT
@@ -555,7 +555,11 @@ inline Splat2D<T> splat2D(const T* pr) {
 
 template <class T>
 inline T pairExponent(const Splat2D<T>& s, T dx, T dy) {
-  return std::fmax(std::fma(T(0.5), std::fma(s.cA * dx, dx, (s.cC * dy) * dy), (s.cB * dx) * dy), T(0));
+  // e = 0.5 cA dx^2 + cB dx dy + 0.5 cC dy^2 evaluated as
+  // fma(fma(cA/2, dx, cB*dy), dx, ((cC/2)*dy)*dy); halving is exact
+  const T hA = T(0.5) * s.cA, hC = T(0.5) * s.cC;
+  const T u = std::fma(hA, dx, s.cB * dy);
+  return std::fmax(std::fma(u, dx, (hC * dy) * dy), T(0));
 }
 
 // Loss of one pixel (shaders.js:589-618).  Returns false for an invalid

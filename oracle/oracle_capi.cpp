@@ -108,7 +108,7 @@ void oracle_records_f32(const OOpts* oo, const OCam* oc, const float* proj, uint
     // the rasteriser's conservative whole-warp cull radius: rad + 1 px, or
     // unbounded when the radius clamp (radClamp * W) was active
     const float cullR = pr[15] >= o.radClamp * (float)c.W ? INFINITY : pr[15] + 1.0f;
-    const float v[12] = {s.mx, s.my, s.cA, s.cB, s.cC, s.w, s.r, s.g, s.b, s.opa, s.cnorm, cullR};
+    const float v[12] = {s.mx, s.my, 0.5f * s.cA, s.cB, 0.5f * s.cC, s.w, s.r, s.g, s.b, s.opa, s.cnorm, cullR};
     for (int k = 0; k < 12; ++k) r[k] = v[k];
     const TileRect t = tileRect<float>(c, o.tile, pr[0], pr[1], pr[15]);
     rect2[2 * i] = (uint32_t)t.x0 | ((uint32_t)t.y0 << 16);

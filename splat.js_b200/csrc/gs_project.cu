@@ -83,8 +83,10 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   // unless the radius was clamped; one pixel of margin covers rounding
   const float cullR = rad >= a.radClamp * (float)c.W ? __int_as_float(0x7F800000) : rad + 1.0f;
   RenderRec r;
-  r.r0 = make_float4(mx, my, cd * inv, -g.vb * inv);
-  r.r1 = make_float4(ad * inv, opa * comp, col[0], col[1]);
+  // conic stored as (cA/2, cB, cC/2): halving is exact and saves the
+  // rasteriser's per-pixel multiplies by 0.5
+  r.r0 = make_float4(mx, my, 0.5f * (cd * inv), -g.vb * inv);
+  r.r1 = make_float4(0.5f * (ad * inv), opa * comp, col[0], col[1]);
   r.r2 = make_float4(col[2], opa, cnorm, cullR);
   a.recs[slot] = r;
   a.depth[slot] = g.pc[2];

@@ -3,8 +3,9 @@
 // (shaders.js:544-700), over a shared (view, tile) work queue.
 //
 // One CTA works on one TILE x TILE tile at a time (TILE = 8, 16 or 32; one
-// thread per pixel; each warp covers an 8x4 block of the tile).  Splat records of the tile's
-// sorted entries are staged in shared memory BATCH at a time.
+// thread per pixel; each warp covers an 8x4 block of the tile).  Splat
+// records of the tile's sorted entries are staged in shared memory BATCH at
+// a time.
 //
 // Forward: front-to-back compositing; the block leaves the tile when
 // __syncthreads_count (a block-wide ballot) finds every pixel saturated.  In
@@ -24,10 +25,15 @@
 // slot, tile).  Integer sums commute, so results are bit-identical in any
 // order -- the deterministic mode is the only mode.
 //
+// Control flow is warp-uniform (votes); per-lane work runs predicated, so
+// no divergent branch needs a reconvergence scaffold in the hot loops.
 // The per-pair arithmetic is the canonical FP32 sequence the CPU
 // restatement performs.  The 2^14 fixed-point scale is folded into upstream
 // factors (galpha, gC): scaling by a power of two is exact, so every
-// truncated integer equals the one the unfolded sequence produces.
+// truncated integer equals the one the unfolded sequence produces.  The
+// +-1e9 clamp is skipped when a warp's scaled galpha is below 1e7: the
+// conic normaliser bounds every slot by 80 |galpha * 2^14| (slots 7-9 by
+// |gC * 2^14|), so the clamp cannot change a value then.
 #include "gs_common.cuh"
 #include "gs_kernels.h"
 
@@ -36,10 +42,10 @@ namespace gs {
 constexpr int MASKW = 128;        // ballot-bit words per warp: entries 0..4095 of a tile
 constexpr uint32_t FULL = 0xFFFFFFFFu;
 
-__device__ __forceinline__ float pairExponent(const float4& r0, float cC, float dx, float dy) {
-  // e = max(fma(0.5, fma(cA*dx, dx, (cC*dy)*dy), (cB*dx)*dy), 0)
-  const float q = __fmaf_rn(r0.z * dx, dx, (cC * dy) * dy);
-  return fmaxf(__fmaf_rn(0.5f, q, (r0.w * dx) * dy), 0.0f);
+// e = max(fma(fma(cA/2, dx, cB*dy), dx, ((cC/2)*dy)*dy), 0); r0 = (mx, my, cA/2, cB)
+__device__ __forceinline__ float pairExponent(const float4& r0, float hC, float dx, float dy) {
+  const float u = __fmaf_rn(r0.z, dx, r0.w * dy);
+  return fmaxf(__fmaf_rn(u, dx, (hC * dy) * dy), 0.0f);
 }
 
 // trunc(clamp(x, -1e9, 1e9)) for an already scaled value
@@ -122,39 +128,40 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
         __syncthreads();
         if (!__all_sync(FULL, done)) {
           const uint32_t rbase = base - s;
-          uint32_t bits = 0;
-          for (uint32_t j = 0; j < nb; ++j) {
-            const float4 r0 = s_rec[j].r0;
-            const float4 r1 = s_rec[j].r1;
-            const float dx = px - r0.x, dy = py - r0.y;
-            const float ee = pairExponent(r0, r1.x, dx, dy);
-            const bool c1 = !done && ee <= E_CUT;
-            // warp-uniform branch; the body runs predicated per lane (lanes
-            // outside the cutoff see a clamped exponent and are masked off)
-            if (__any_sync(FULL, c1)) {
-              const float araw = r1.y * gexp(-fminf(ee, 80.0f));
-              const float alpha = fminf(0.99f, araw);
-              const bool c2 = c1 && alpha >= A_MIN;
-              if (STORED && c2) a.tStore[(size_t)(base + j) * RTHREADS + tid] = T;
-              const float ta = T * alpha;
-              const float cb = s_rec[j].r2.x;
-              if (c2) {
-                C0 = __fmaf_rn(ta, r1.z, C0);
-                C1 = __fmaf_rn(ta, r1.w, C1);
-                C2 = __fmaf_rn(ta, cb, C2);
-                T = T * (1.0f - alpha);
-                if (T < 1e-4f) { done = true; cnt = rbase + j + 1; }
+          for (uint32_t jw = 0; jw < nb; jw += 32) {  // one ballot word per 32 entries
+            const uint32_t jn = min(32u, nb - jw);
+            uint32_t bits = 0;
+            for (uint32_t jj = 0; jj < jn; ++jj) {
+              const RenderRec& rr = s_rec[jw + jj];
+              const float4 r0 = rr.r0;
+              const float4 r1 = rr.r1;
+              const float dx = px - r0.x, dy = py - r0.y;
+              const float ee = pairExponent(r0, r1.x, dx, dy);
+              const bool c1 = !done && ee <= E_CUT;
+              // warp-uniform branch; the body runs predicated per lane (lanes
+              // outside the cutoff see a clamped exponent and are masked off)
+              if (__any_sync(FULL, c1)) {
+                const float araw = r1.y * gexp(-fminf(ee, 80.0f));
+                const float alpha = fminf(0.99f, araw);
+                const bool c2 = c1 && alpha >= A_MIN;
+                if (STORED && c2) a.tStore[(size_t)(base + jw + jj) * RTHREADS + tid] = T;
+                const float ta = T * alpha;
+                const float cb = rr.r2.x;
+                if (c2) {
+                  C0 = __fmaf_rn(ta, r1.z, C0);
+                  C1 = __fmaf_rn(ta, r1.w, C1);
+                  C2 = __fmaf_rn(ta, cb, C2);
+                  T = T * (1.0f - alpha);
+                  if (T < 1e-4f) { done = true; cnt = rbase + jw + jj + 1; }
+                }
+                if (MASKS) bits |= (__ballot_sync(FULL, c2) != 0u ? 1u : 0u) << jj;
               }
-              if (MASKS) bits |= (__ballot_sync(FULL, c2) != 0u ? 1u : 0u) << (j & 31);
             }
-            if ((j & 31) == 31 || j + 1 == nb) {  // word boundary: store bits, leave when all saturated
-              if (MASKS) {
-                const uint32_t w = (rbase + j) >> 5;
-                if (lane == 0 && w < MASKW) wmask[w] = bits;
-                bits = 0;
-              }
-              if (__all_sync(FULL, done)) break;
+            if (MASKS) {
+              const uint32_t w = (rbase + jw) >> 5;
+              if (lane == 0 && w < MASKW) wmask[w] = bits;
             }
+            if (__all_sync(FULL, done)) break;
           }
         }
         __syncthreads();
@@ -206,6 +213,8 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
           cg7 = fixq(eg0 + eg1 + eg2, FIXCAM);
         }
       }
+      // slots 7-9 stay within +-1e9 without clamping when |gC * 2^14| < 9e8
+      const bool pixFast = fabsf(g16_0) < 9.0e8f && fabsf(g16_1) < 9.0e8f && fabsf(g16_2) < 9.0e8f;
       // block sums of the per-pixel stats (wrapping u32 / i32, as the
       // reference's atomics) and the largest end index of the tile
       const uint32_t myEnd = lossOk ? cnt : 0u;
@@ -248,37 +257,34 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
           s_rec[k] = recs[id];
         }
         __syncthreads();
-        // this warp's entries in [lo, hi), back to front
-        int32_t jn = (int32_t)hi - 1;
-        while (jn >= (int32_t)lo) {
-          uint32_t j = (uint32_t)jn;
-          if (MASKS && j < (uint32_t)MASKW * 32u) {
-            const uint32_t w = j >> 5;
-            uint32_t word = wmask[w] & (FULL >> (31u - (j & 31u)));
-            if ((w << 5) < lo) word &= ~((1u << (lo & 31u)) - 1u);
-            if (word == 0u) { jn = (int32_t)(w << 5) - 1; continue; }
-            j = (w << 5) + 31u - (uint32_t)__clz(word);
-          } else if (!warpTouches(s_rec[j - lo].r0, s_rec[j - lo].r2.w, wcx, wcy)) {
-            jn = (int32_t)j - 1;
-            continue;
-          }
-          jn = (int32_t)j - 1;
-          // Straight-line body, predicated per lane: lanes that do not
-          // composite this entry (past their end, outside a cutoff) compute
-          // on a clamped exponent and have their contribution zeroed through
-          // galpha and aT, and keep S and Ta.  Composing lanes perform
-          // exactly the canonical sequence.
-          const RenderRec& rr = s_rec[j - lo];
-          const float4 r0 = rr.r0;
-          const float4 r1 = rr.r1;
-          const float4 r2 = rr.r2;
-          const float dx = px - r0.x, dy = py - r0.y;
-          const float ee = pairExponent(r0, r1.x, dx, dy);
-          const float G = gexp(-fminf(ee, 80.0f));
-          const float araw = r1.y * G;
-          const float alpha = fminf(0.99f, araw);
-          const bool c2 = j < myEnd && ee <= E_CUT && alpha >= A_MIN;
-          if (__any_sync(FULL, c2)) {
+        // this warp's entries in [lo, hi), back to front, one ballot word at a time
+        for (int32_t w = (int32_t)((hi - 1) >> 5); w >= (int32_t)(lo >> 5); --w) {
+          const uint32_t wb = (uint32_t)w << 5;
+          const bool haveBits = MASKS && (uint32_t)w < (uint32_t)MASKW;
+          uint32_t word = haveBits ? wmask[w] : FULL;
+          if (wb + 32u > hi) word &= FULL >> (wb + 32u - hi);
+          if (wb < lo) word &= FULL << (lo - wb);
+          while (word) {
+            const uint32_t bit = 31u - (uint32_t)__clz(word);
+            word &= ~(1u << bit);
+            const uint32_t j = wb + bit;
+            const RenderRec& rr = s_rec[j - lo];
+            const float4 r0 = rr.r0;
+            const float4 r1 = rr.r1;
+            const float4 r2 = rr.r2;
+            if (!haveBits && !warpTouches(r0, r2.w, wcx, wcy)) continue;
+            // Straight-line body, predicated per lane: lanes that do not
+            // composite this entry (past their end, outside a cutoff) compute
+            // on a clamped exponent and have their contribution zeroed
+            // through galpha and aT, and keep S and Ta.  Compositing lanes
+            // perform exactly the canonical sequence.
+            const float dx = px - r0.x, dy = py - r0.y;
+            const float ee = pairExponent(r0, r1.x, dx, dy);
+            const float G = gexp(-fminf(ee, 80.0f));
+            const float araw = r1.y * G;
+            const float alpha = fminf(0.99f, araw);
+            const bool c2 = j < myEnd && ee <= E_CUT && alpha >= A_MIN;
+            if (!__any_sync(FULL, c2)) continue;
             const float inv = __frcp_rn(1.0f - alpha);
             const float Tb = STORED ? (c2 ? a.tStore[(size_t)(s + j) * RTHREADS + tid] : 0.0f) : Ta * inv;
             const float aT = c2 ? alpha * Tb : 0.0f;
@@ -289,19 +295,28 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
             if (araw > 0.99f) galpha = 0.0f;
             const float gal16 = c2 ? galpha * FIXED : 0.0f;
             const float ga16 = gal16 * araw;
+            const float cA = r0.z + r0.z, cC = r1.x + r1.x;  // exact doubling of the stored halves
             const float gq16 = ga16 * (-0.5f * r2.z);
             const float gqx16 = gq16 * dx;
-            uint32_t r[10];
-            r[0] = __reduce_add_sync(FULL, (uint32_t)fix_scaled(ga16 * __fmaf_rn(r0.z, dx, r0.w * dy)));
-            r[1] = __reduce_add_sync(FULL, (uint32_t)fix_scaled(ga16 * __fmaf_rn(r0.w, dx, r1.x * dy)));
-            r[2] = __reduce_add_sync(FULL, (uint32_t)fix_scaled(gqx16 * dx));
-            r[3] = __reduce_add_sync(FULL, (uint32_t)fix_scaled((gqx16 * dy) * 2.0f));
-            r[4] = __reduce_add_sync(FULL, (uint32_t)fix_scaled((gq16 * dy) * dy));
-            r[5] = __reduce_add_sync(FULL, (uint32_t)fix_scaled((gal16 * r2.y) * G));
-            r[6] = __reduce_add_sync(FULL, (uint32_t)fix_scaled(ga16 * (1.0f - r2.y)));
-            r[7] = __reduce_add_sync(FULL, (uint32_t)fix_scaled(g16_0 * aT));
-            r[8] = __reduce_add_sync(FULL, (uint32_t)fix_scaled(g16_1 * aT));
-            r[9] = __reduce_add_sync(FULL, (uint32_t)fix_scaled(g16_2 * aT));
+            float xs[10];
+            xs[0] = ga16 * __fmaf_rn(cA, dx, r0.w * dy);
+            xs[1] = ga16 * __fmaf_rn(r0.w, dx, cC * dy);
+            xs[2] = gqx16 * dx;
+            xs[3] = (gqx16 * dy) * 2.0f;
+            xs[4] = (gq16 * dy) * dy;
+            xs[5] = (gal16 * r2.y) * G;
+            xs[6] = ga16 * (1.0f - r2.y);
+            xs[7] = g16_0 * aT;
+            xs[8] = g16_1 * aT;
+            xs[9] = g16_2 * aT;
+            uint32_t rsum[10];
+            if (__all_sync(FULL, fabsf(gal16) < 1.0e7f && pixFast)) {
+#pragma unroll
+              for (int k = 0; k < 10; ++k) rsum[k] = __reduce_add_sync(FULL, (uint32_t)__float2int_rz(xs[k]));
+            } else {
+#pragma unroll
+              for (int k = 0; k < 10; ++k) rsum[k] = __reduce_add_sync(FULL, (uint32_t)fix_scaled(xs[k]));
+            }
             if (c2) {
               S0 = __fmaf_rn(r1.z, aT, S0);
               S1 = __fmaf_rn(r1.w, aT, S1);
@@ -311,8 +326,7 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
             if (lane == 0) {
               int32_t* acc = s_acc + (j - lo) * 10;
 #pragma unroll
-              for (int k = 0; k < 10; ++k)
-                if (r[k]) atomicAdd(&acc[k], (int32_t)r[k]);
+              for (int k = 0; k < 10; ++k) atomicAdd(&acc[k], (int32_t)rsum[k]);
             }
           }
         }
