@@ -12,18 +12,18 @@
 // the fused train kernel each warp also records, per entry, whether any of
 // its pixels composited it (a ballot bit in shared memory): on dense scenes
 // only about a fifth of warp-entries composite anything.
-// Backward: each warp walks only the entries its bits mark, back to front,
-// with no block barrier (without bits -- backward from saved state, or
-// entries past the bit capacity -- a warp-uniform test against the splat's
-// conservative radius, rad + 1 px, skips entries that cannot reach the
-// warp's 8x4 pixels); each pixel recovers the transmittance in front of a
-// splat from the final one (Tb = Ta / (1 - alpha)) -- or, in the
-// stored-state variant, reads the value the forward saved.  The ten gradient
-// contributions of each pixel are truncated to i32 fixed point (the
-// reference's i32(clamp(v*16384, +-1e9))) and summed exactly: a warp REDUX
-// per slot, then one global atomic per (splat, slot, warp).  Integer sums
-// commute, so results are bit-identical in any order -- the deterministic
-// mode is the only mode.
+// Backward: each warp walks only the entries its bits mark, back to front
+// (without bits -- backward from saved state, or entries past the bit
+// capacity -- a warp-uniform test against the splat's conservative radius,
+// rad + 1 px, skips entries that cannot reach the warp's 8x4 pixels);
+// each pixel recovers the transmittance in front of a splat from the final
+// one (Tb = Ta / (1 - alpha)) -- or, in the stored-state variant, reads the
+// value the forward saved.  The ten gradient contributions of each pixel are
+// truncated to i32 fixed point (the reference's i32(clamp(v*16384, +-1e9)))
+// and summed exactly: a warp REDUX per slot, a shared-memory add per
+// (entry, slot) across the tile's warps, and one global atomic per (splat,
+// slot, tile).  Integer sums commute, so results are bit-identical in any
+// order -- the deterministic mode is the only mode.
 //
 // Control flow is warp-uniform (votes); per-lane work runs predicated, so
 // no divergent branch needs a reconvergence scaffold in the hot loops.
@@ -68,6 +68,8 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
   constexpr bool MASKS = FWD && BWD;
   static_assert(BATCH % 32 == 0, "batches hold whole ballot words");
   __shared__ RenderRec s_rec[BATCH];
+  __shared__ uint32_t s_id[BATCH];
+  __shared__ int32_t s_acc[BWD ? BATCH * 10 : 1];
   __shared__ uint32_t s_mask[MASKS ? NW * MASKW : 1];
   __shared__ uint32_t s_item;
   __shared__ uint32_t s_redu[NW][5];
@@ -78,6 +80,9 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
   const int ly = (wid / WPR) * 4 + (lane >> 3);
   const float E_CUT = a.eCut, A_MIN = a.aMin;
   uint32_t* wmask = s_mask + (MASKS ? wid * MASKW : 0);
+
+  if (BWD)
+    for (int k = tid; k < BATCH * 10; k += RTHREADS) s_acc[k] = 0;
 
   for (uint32_t iter = 0;; ++iter) {
     // ---- next work item (a global tile of the batch) ----
@@ -115,7 +120,11 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
       for (uint32_t base = s; base < e; base += BATCH) {
         if (__syncthreads_count(!done) == 0) break;
         const uint32_t nb = min((uint32_t)BATCH, e - base);
-        for (uint32_t k = tid; k < nb; k += RTHREADS) s_rec[k] = recs[a.ids[base + k]];
+        for (uint32_t k = tid; k < nb; k += RTHREADS) {
+          const uint32_t id = a.ids[base + k];
+          s_id[k] = id;
+          s_rec[k] = recs[id];
+        }
         __syncthreads();
         if (!__all_sync(FULL, done)) {
           const uint32_t rbase = base - s;
@@ -231,51 +240,38 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
           else atomicAdd(&a.gradCam[c.camIdx * 8u + 3u + (uint32_t)tid], (int32_t)sum);
         }
       }
+      uint32_t endMax = 0;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) endMax = max(endMax, s_endmax[w]);
       // ---- backward (shaders.js:632-700) ----
-      // Barrier-free: each warp walks its own ballot bits back to front from
-      // the largest end index among its pixels, loading each marked entry's
-      // id and record straight from global memory (warp-uniform loads of
-      // L2-resident data, the next entry's id fetched one step ahead), and
-      // adds its warp-reduced sums to the splat's accumulators in global
-      // memory.
-      const uint32_t wEnd = s_endmax[wid];
       float S0 = c.bg[0] * T, S1 = c.bg[1] * T, S2 = c.bg[2] * T;
       float Ta = T;
       int32_t* gradP = a.gradP + (size_t)v * a.n * GP_STRIDE;
-      const uint32_t* tids = a.ids + s;
-      if (wEnd > 0) {
-        int32_t w = (int32_t)((wEnd - 1) >> 5);
-        auto wordAt = [&](int32_t ww) -> uint32_t {
-          uint32_t wd = (MASKS && (uint32_t)ww < (uint32_t)MASKW) ? wmask[ww] : FULL;
-          const uint32_t wb = (uint32_t)ww << 5;
-          if (wb + 32u > wEnd) wd &= FULL >> (wb + 32u - wEnd);
-          return wd;
-        };
-        uint32_t word = wordAt(w);
-        // advance to the next marked entry (j = ~0 when none is left)
-        auto nextEntry = [&]() -> uint32_t {
-          while (word == 0u) {
-            if (--w < 0) return 0xFFFFFFFFu;
-            word = wordAt(w);
-          }
-          const uint32_t bit = 31u - (uint32_t)__clz(word);
-          word &= ~(1u << bit);
-          return ((uint32_t)w << 5) + bit;
-        };
-        uint32_t j = nextEntry();
-        uint32_t idCur = j != 0xFFFFFFFFu ? __ldg(tids + j) : 0u;
-        while (j != 0xFFFFFFFFu) {
-          const uint32_t jNext = nextEntry();
-          const uint32_t idNext = jNext != 0xFFFFFFFFu ? __ldg(tids + jNext) : 0u;
-          const uint32_t id = idCur;
-          const uint32_t jc = j;
-          j = jNext;
-          idCur = idNext;
-          const float4 r0 = __ldg(&recs[id].r0);
-          const float4 r1 = __ldg(&recs[id].r1);
-          const float4 r2 = __ldg(&recs[id].r2);
-          {
-            const bool haveBits = MASKS && jc < (uint32_t)MASKW * 32u;
+      for (uint32_t hi = endMax; hi > 0;) {
+        const uint32_t lo = hi > (uint32_t)BATCH ? hi - BATCH : 0u;
+        const uint32_t nb = hi - lo;
+        __syncthreads();
+        for (uint32_t k = tid; k < nb; k += RTHREADS) {
+          const uint32_t id = a.ids[s + lo + k];
+          s_id[k] = id;
+          s_rec[k] = recs[id];
+        }
+        __syncthreads();
+        // this warp's entries in [lo, hi), back to front, one ballot word at a time
+        for (int32_t w = (int32_t)((hi - 1) >> 5); w >= (int32_t)(lo >> 5); --w) {
+          const uint32_t wb = (uint32_t)w << 5;
+          const bool haveBits = MASKS && (uint32_t)w < (uint32_t)MASKW;
+          uint32_t word = haveBits ? wmask[w] : FULL;
+          if (wb + 32u > hi) word &= FULL >> (wb + 32u - hi);
+          if (wb < lo) word &= FULL << (lo - wb);
+          while (word) {
+            const uint32_t bit = 31u - (uint32_t)__clz(word);
+            word &= ~(1u << bit);
+            const uint32_t j = wb + bit;
+            const RenderRec& rr = s_rec[j - lo];
+            const float4 r0 = rr.r0;
+            const float4 r1 = rr.r1;
+            const float4 r2 = rr.r2;
             if (!haveBits && !warpTouches(r0, r2.w, wcx, wcy)) continue;
             // Straight-line body, predicated per lane: lanes that do not
             // composite this entry (past their end, outside a cutoff) compute
@@ -287,10 +283,10 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
             const float G = gexp(-fminf(ee, 80.0f));
             const float araw = r1.y * G;
             const float alpha = fminf(0.99f, araw);
-            const bool c2 = jc < myEnd && ee <= E_CUT && alpha >= A_MIN;
+            const bool c2 = j < myEnd && ee <= E_CUT && alpha >= A_MIN;
             if (!__any_sync(FULL, c2)) continue;
             const float inv = __frcp_rn(1.0f - alpha);
-            const float Tb = STORED ? (c2 ? a.tStore[(size_t)(s + jc) * RTHREADS + tid] : 0.0f) : Ta * inv;
+            const float Tb = STORED ? (c2 ? a.tStore[(size_t)(s + j) * RTHREADS + tid] : 0.0f) : Ta * inv;
             const float aT = c2 ? alpha * Tb : 0.0f;
             const float g0 = __fmaf_rn(r1.z, Tb, -(S0 * inv));
             const float g1 = __fmaf_rn(r1.w, Tb, -(S1 * inv));
@@ -328,13 +324,22 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
               Ta = Tb;
             }
             if (lane == 0) {
-              int32_t* acc = gradP + (size_t)id * GP_STRIDE;
+              int32_t* acc = s_acc + (j - lo) * 10;
 #pragma unroll
-              for (int k = 0; k < 10; ++k)
-                if (rsum[k]) atomicAdd(&acc[k], (int32_t)rsum[k]);
+              for (int k = 0; k < 10; ++k) atomicAdd(&acc[k], (int32_t)rsum[k]);
             }
           }
         }
+        __syncthreads();
+        for (uint32_t k = tid; k < nb * 10; k += RTHREADS) {
+          const int32_t val = s_acc[k];
+          if (val) {
+            const uint32_t jl = k / 10, slot = k - jl * 10;
+            atomicAdd(&gradP[(size_t)s_id[jl] * GP_STRIDE + slot], val);
+            s_acc[k] = 0;
+          }
+        }
+        hi = lo;
       }
     }
     __syncthreads();
