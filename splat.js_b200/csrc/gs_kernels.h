@@ -17,7 +17,8 @@ struct ProjectArgs {
   float eCut, aMin, radClamp;
   int tile;
   RenderRec* recs;         // V * n
-  float* depth;            // V * n camera-space depth (sort key)
+  uint64_t* pkeys;         // V * n presort keys: view << 32 | depth bits (all ones when culled)
+  uint32_t* pvals;         // V * n presort values: slot = view * n + splat
   uint2* rect;             // V * n
   int32_t* diffGrid;       // per view (tilesX+1)*(tilesY+1), cleared before
   const uint32_t* gridBase;  // V offsets into diffGrid
@@ -32,6 +33,7 @@ struct TileRangeArgs {
   uint8_t* dropped;        // per global tile: dropped by the entry budget
   uint2* ranges;           // per global tile: [start, end) in the sorted entries
   uint32_t* viewDrops;     // per view: number of dropped tiles
+  uint32_t* viewTotal;     // per view: kept entries
   uint32_t* stats;         // stats[3] += dropped tiles
   uint64_t entriesCap;     // per-view entry budget (ENTCAP)
   uint32_t* totalEntries;  // out: kept entries over the batch
@@ -41,29 +43,30 @@ struct SplatCountArgs {
   uint32_t n;
   int V;
   const DevCam* cams;
+  const uint32_t* sortedSlots;  // presorted (view, depth, id) order
   const uint2* rect;
   const uint8_t* dropped;
   const uint32_t* viewDrops;
-  uint32_t* counts;        // V * n
+  uint32_t* counts;        // V * n, in presorted order
 };
 
 struct KeygenArgs {
   uint32_t n;
   int V;
   const DevCam* cams;
+  const uint32_t* sortedSlots;
   const uint2* rect;
-  const float* depth;
   const uint8_t* dropped;
   const uint32_t* viewDrops;
-  const uint32_t* offsets;  // V * n exclusive scan of counts
-  uint64_t* keys;
-  uint32_t* vals;
+  const uint32_t* offsets;  // V * n exclusive scan of counts (presorted order)
+  uint32_t* keys;           // global tile id per entry
+  uint32_t* vals;           // splat id per entry
   uint64_t capacity;
   uint32_t* status;
 };
 
 struct RadixHistArgs {
-  const uint64_t* keys;
+  const void* keys;        // uint32_t or uint64_t
   const uint32_t* nItems;
   uint32_t* hist;           // passes * 256
   int passes;
@@ -71,9 +74,9 @@ struct RadixHistArgs {
 };
 
 struct OnesweepArgs {
-  const uint64_t* keysIn;
+  const void* keysIn;
   const uint32_t* valsIn;
-  uint64_t* keysOut;        // null: do not write keys (last pass)
+  void* keysOut;            // null: do not write keys (last pass)
   uint32_t* valsOut;
   const uint32_t* nItems;
   const uint32_t* hist;
@@ -85,7 +88,8 @@ struct OnesweepArgs {
 };
 
 struct RadixSortArgs {
-  uint64_t* keys[2];
+  void* keys[2];            // ping-pong key buffers of keyBytes-wide keys
+  int keyBytes;             // 4 or 8
   uint32_t* vals[2];
   const uint32_t* nItems;
   uint32_t* hist;
@@ -171,7 +175,7 @@ struct RefineApplyArgs {
 
 // launchers
 void launch_project(const ProjectArgs& a, int deg, cudaStream_t s);
-void launch_tile_ranges(const TileRangeArgs& a, cudaStream_t s);
+void launch_tile_ranges(const TileRangeArgs& a, uint32_t totalTiles, cudaStream_t s);
 void launch_splat_counts(const SplatCountArgs& a, cudaStream_t s);
 void launch_keygen(const KeygenArgs& a, cudaStream_t s);
 uint32_t scan_partials_needed(uint64_t N);

@@ -1,30 +1,38 @@
 // gs_project.cu -- pass 1 of the training step: projection + SH colour
-// (shaders.js:228-315), for every (view, splat) of a batch in one launch.
+// (shaders.js:228-315) for every (view, splat) of a batch, and the binning
+// that turns projected splats into sorted per-tile entry lists.
 //
-// Outputs per (view, splat):
-//   RenderRec  the 48-byte record the rasteriser stages (mean, conic,
-//              opacity*comp, colour, opacity, conic normaliser, depth);
-//   rect       tile bounds packed as {x0 | y0<<16, x1 | y1<<16}, or
-//              {0xFFFFFFFF, 0} when culled (the reference's visible flag);
-// and four atomic adds into the view's tile "difference grid", whose 2D
-// prefix sum is the reference's per-tile count tileCnt (shaders.js:303-313)
-// at 4 atomics per splat instead of one per covered tile.
+// Binning.  The reference counts tiles per splat, scans, scatters (key, id)
+// pairs into per-tile segments with atomic cursors and bitonic-sorts each
+// segment by (depth f32 bits, id) (shaders.js:303-500).  Here:
+//   1. k_project writes, per (view, splat), the raster record, the tile
+//      rectangle, four atomics into the view's tile difference grid (its 2D
+//      prefix sum is the reference's per-tile count), and a presort item:
+//      key (view << 32 | depth bits) -- all ones when culled -- and value
+//      slot = view * n + splat;
+//   2. k_tile_counts (one block per view): tileCnt, the reference's entry
+//      budget (drops), and view-local tile ranges; k_tile_ranges_finish
+//      offsets them by the earlier views' totals;
+//   3. the items are radix-sorted by key (stable, so equal depths keep id
+//      order): (view, depth, id) order;
+//   4. k_splat_counts / scan / k_keygen expand the sorted items into one
+//      entry per (splat, tile) -- key = global tile id (32 bits), value =
+//      splat id -- written in that order;
+//   5. a stable radix sort on the tile id leaves every tile's entries in
+//      (depth bits, id) order: the reference's per-tile order, with two
+//      passes over 8-byte entries instead of six over 12-byte ones.
 #include "gs_geom.cuh"
 #include "gs_kernels.h"
 
 namespace gs {
 
+// One thread per splat, looping over the batch's views: parameters and SH
+// coefficients are read once per step.
 template <int DEG>
 __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   constexpr int K = DEG > 0 ? (DEG + 1) * (DEG + 1) - 1 : 0;
-  const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= (uint64_t)a.n * a.V) return;
-  const uint32_t v = (uint32_t)(gid / a.n);
-  const uint32_t i = (uint32_t)(gid - (uint64_t)v * a.n);
-  const DevCam c = a.cams[v];
-  const size_t slot = (size_t)v * a.n + i;
-  a.rect[slot] = make_uint2(0xFFFFFFFFu, 0u);
-
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
   float P[16];
   const float4* P4 = reinterpret_cast<const float4*>(a.params + (size_t)i * STRIDE);
 #pragma unroll
@@ -32,196 +40,214 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
     const float4 t = P4[k];
     P[4 * k] = t.x; P[4 * k + 1] = t.y; P[4 * k + 2] = t.z; P[4 * k + 3] = t.w;
   }
-  const Geom g = computeGeom(c, P);
-  if (!g.ok) return;
-  const float detV = fmaxf(g.va * g.vc - g.vb * g.vb, 0.0f);
-  const float ad = g.va + 0.3f, cd = g.vc + 0.3f;
-  const float detVd = ad * cd - g.vb * g.vb;
-  if (detVd < 1e-8f) return;
-  const float comp = sqrtf(fmaxf(detV / detVd, 0.0f));
+  const float* shp = K > 0 ? a.sh + (size_t)i * 3 * K : nullptr;
+  const float sig0 = sigm(P[10]), sig1 = sigm(P[11]), sig2 = sigm(P[12]);
   const float opa = sigm(P[13]);
-  if (opa * comp < a.aMin) return;
-  const float f = c.f;
-  const float mx = f * g.pc[0] / g.pc[2] + c.cx;
-  const float my = f * g.pc[1] / g.pc[2] + c.cy;
-  const float mid = 0.5f * (ad + cd);
-  const float disc = sqrtf(fmaxf(mid * mid - detVd, 0.0f));
-  const float eMax = fminf(a.eCut, glog(fmaxf(opa * comp / a.aMin, 1.0001f)));
-  const float rad = fminf(sqrtf(2.0f * eMax) * sqrtf(mid + disc), a.radClamp * (float)c.W);
-  const float W = (float)c.W, H = (float)c.H;
-  if (mx + rad < 0.0f || my + rad < 0.0f || mx - rad > W || my - rad > H) return;
-  const float inv = 1.0f / detVd;
-  float col[3] = {sigm(P[10]), sigm(P[11]), sigm(P[12])};
-  if (K > 0) {
-    float cp[3];
-    camPosWorld(c, cp);
-    const float un[3] = {P[0] - cp[0], P[1] - cp[1], P[2] - cp[2]};
-    const float len = fmaxf(sqrtf(dot3(un, un)), 1e-9f);
-    const float vd[3] = {un[0] / len, un[1] / len, un[2] / len};
-    float Y[15];
-    shBasis<DEG>(vd, Y);
-    const int aK = shActiveK(c, K);
-    const float* shp = a.sh + (size_t)i * 3 * K;
+
+  for (int v = 0; v < a.V; ++v) {
+    const DevCam& c = a.cams[v];
+    const size_t slot = (size_t)v * a.n + i;
+    a.rect[slot] = make_uint2(0xFFFFFFFFu, 0u);
+    a.pkeys[slot] = ~0ull;
+    a.pvals[slot] = (uint32_t)slot;
+    const Geom g = computeGeom(c, P);
+    if (!g.ok) continue;
+    const float detV = fmaxf(g.va * g.vc - g.vb * g.vb, 0.0f);
+    const float ad = g.va + 0.3f, cd = g.vc + 0.3f;
+    const float detVd = ad * cd - g.vb * g.vb;
+    if (detVd < 1e-8f) continue;
+    const float comp = sqrtf(fmaxf(detV / detVd, 0.0f));
+    if (opa * comp < a.aMin) continue;
+    const float f = c.f;
+    const float mx = f * g.pc[0] / g.pc[2] + c.cx;
+    const float my = f * g.pc[1] / g.pc[2] + c.cy;
+    const float mid = 0.5f * (ad + cd);
+    const float disc = sqrtf(fmaxf(mid * mid - detVd, 0.0f));
+    const float eMax = fminf(a.eCut, glog(fmaxf(opa * comp / a.aMin, 1.0001f)));
+    const float rad = fminf(sqrtf(2.0f * eMax) * sqrtf(mid + disc), a.radClamp * (float)c.W);
+    const float W = (float)c.W, H = (float)c.H;
+    if (mx + rad < 0.0f || my + rad < 0.0f || mx - rad > W || my - rad > H) continue;
+    const float inv = 1.0f / detVd;
+    float col[3] = {sig0, sig1, sig2};
+    if (K > 0) {
+      float cp[3];
+      camPosWorld(c, cp);
+      const float un[3] = {P[0] - cp[0], P[1] - cp[1], P[2] - cp[2]};
+      const float len = fmaxf(sqrtf(dot3(un, un)), 1e-9f);
+      const float vd[3] = {un[0] / len, un[1] / len, un[2] / len};
+      float Y[15];
+      shBasis<DEG>(vd, Y);
+      const int aK = shActiveK(c, K);
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      if (k < aK) {
-        col[0] = col[0] + shp[k] * Y[k];
-        col[1] = col[1] + shp[K + k] * Y[k];
-        col[2] = col[2] + shp[2 * K + k] * Y[k];
+      for (int k = 0; k < K; ++k) {
+        if (k < aK) {
+          col[0] = col[0] + __ldg(shp + k) * Y[k];
+          col[1] = col[1] + __ldg(shp + K + k) * Y[k];
+          col[2] = col[2] + __ldg(shp + 2 * K + k) * Y[k];
+        }
       }
-    }
 #pragma unroll
-    for (int j = 0; j < 3; ++j) col[j] = fmaxf(col[j], 0.0f);
+      for (int j = 0; j < 3; ++j) col[j] = fmaxf(col[j], 0.0f);
+    }
+    // conic normaliser 1/(1 + lambda_max) (shaders.js:674-678); the same value
+    // as 1/(1 + (mid + disc)) computed here from identical operands
+    const float lmax = mid + disc;
+    const float cnorm = 1.0f / (1.0f + lmax);
+    // conservative cull radius for whole warps of pixels: beyond `rad` from the
+    // mean no pixel passes both cutoffs (e >= d^2 / (2 lambda_max) > eMax),
+    // unless the radius was clamped; one pixel of margin covers rounding
+    const float cullR = rad >= a.radClamp * (float)c.W ? __int_as_float(0x7F800000) : rad + 1.0f;
+    RenderRec r;
+    // conic stored as (cA/2, cB, cC/2): halving is exact and saves the
+    // rasteriser's per-pixel multiplies by 0.5
+    r.r0 = make_float4(mx, my, 0.5f * (cd * inv), -g.vb * inv);
+    r.r1 = make_float4(0.5f * (ad * inv), opa * comp, col[0], col[1]);
+    r.r2 = make_float4(col[2], opa, cnorm, cullR);
+    a.recs[slot] = r;
+    a.pkeys[slot] = ((unsigned long long)v << 32) | __float_as_uint(g.pc[2]);
+
+    // tile bounds (shaders.js:303-308)
+    const int tx = c.tilesX, ty = c.tilesY;
+    const float TF = (float)a.tile;
+    const uint32_t x0 = u32sat(clampf(floorf((mx - rad) / TF), 0.0f, (float)(tx - 1)));
+    const uint32_t x1 = u32sat(clampf(floorf((mx + rad) / TF), 0.0f, (float)(tx - 1)));
+    const uint32_t y0 = u32sat(clampf(floorf((my - rad) / TF), 0.0f, (float)(ty - 1)));
+    const uint32_t y1 = u32sat(clampf(floorf((my + rad) / TF), 0.0f, (float)(ty - 1)));
+    a.rect[slot] = make_uint2(x0 | (y0 << 16), x1 | (y1 << 16));
+    // rectangle add on the (tx+1) x (ty+1) difference grid
+    int32_t* gd = a.diffGrid + a.gridBase[v];
+    const int gw = tx + 1;
+    atomicAdd(&gd[y0 * gw + x0], 1);
+    atomicAdd(&gd[y0 * gw + x1 + 1], -1);
+    atomicAdd(&gd[(y1 + 1) * gw + x0], -1);
+    atomicAdd(&gd[(y1 + 1) * gw + x1 + 1], 1);
   }
-  // conic normaliser 1/(1 + lambda_max) (shaders.js:674-678); the same value
-  // as 1/(1 + (mid + disc)) computed here from identical operands
-  const float lmax = mid + disc;
-  const float cnorm = 1.0f / (1.0f + lmax);
-
-  // conservative cull radius for whole warps of pixels: beyond `rad` from the
-  // mean no pixel passes both cutoffs (e >= d^2 / (2 lambda_max) > eMax),
-  // unless the radius was clamped; one pixel of margin covers rounding
-  const float cullR = rad >= a.radClamp * (float)c.W ? __int_as_float(0x7F800000) : rad + 1.0f;
-  RenderRec r;
-  // conic stored as (cA/2, cB, cC/2): halving is exact and saves the
-  // rasteriser's per-pixel multiplies by 0.5
-  r.r0 = make_float4(mx, my, 0.5f * (cd * inv), -g.vb * inv);
-  r.r1 = make_float4(0.5f * (ad * inv), opa * comp, col[0], col[1]);
-  r.r2 = make_float4(col[2], opa, cnorm, cullR);
-  a.recs[slot] = r;
-  a.depth[slot] = g.pc[2];
-
-  // tile bounds (shaders.js:303-308)
-  const int tx = c.tilesX, ty = c.tilesY;
-  const float TF = (float)a.tile;
-  const uint32_t x0 = u32sat(clampf(floorf((mx - rad) / TF), 0.0f, (float)(tx - 1)));
-  const uint32_t x1 = u32sat(clampf(floorf((mx + rad) / TF), 0.0f, (float)(tx - 1)));
-  const uint32_t y0 = u32sat(clampf(floorf((my - rad) / TF), 0.0f, (float)(ty - 1)));
-  const uint32_t y1 = u32sat(clampf(floorf((my + rad) / TF), 0.0f, (float)(ty - 1)));
-  a.rect[slot] = make_uint2(x0 | (y0 << 16), x1 | (y1 << 16));
-  // rectangle add on the (tx+1) x (ty+1) difference grid
-  int32_t* gd = a.diffGrid + a.gridBase[v];
-  const int gw = tx + 1;
-  atomicAdd(&gd[y0 * gw + x0], 1);
-  atomicAdd(&gd[y0 * gw + x1 + 1], -1);
-  atomicAdd(&gd[(y1 + 1) * gw + x0], -1);
-  atomicAdd(&gd[(y1 + 1) * gw + x1 + 1], 1);
 }
 
-// One CTA per batch: per view, the 2D prefix sum of the difference grid gives
-// the reference's tileCnt; then the budgeted scan of shaders.js:341-372 with
+// One block (1024 threads) per view: the 2D prefix sum of the difference grid
+// gives the reference's tileCnt; the budgeted scan of shaders.js:341-372 with
 // its padding rule (segments above 2048 entries round up to a power of two)
 // decides which tiles the entry budget drops (counted in stats[3]); the
-// kept counts' exclusive scan over (view, tile) is each tile's range in the
-// sorted entry list.  Views are processed in order so ranges are global.
-__global__ void __launch_bounds__(1024) k_tile_ranges(TileRangeArgs a) {
-  __shared__ uint32_t s_base;
-  __shared__ uint32_t s_red[32];
-  if (threadIdx.x == 0) s_base = 0;
+// kept counts' exclusive scan gives view-local tile ranges.
+__global__ void __launch_bounds__(1024) k_tile_counts(TileRangeArgs a) {
+  __shared__ uint32_t s_red[33];
+  const int v = blockIdx.x;
+  const DevCam c = a.cams[v];
+  const int tx = c.tilesX, ty = c.tilesY, gw = tx + 1;
+  int32_t* gd = a.diffGrid + a.gridBase[v];
+  // rows: prefix along x
+  for (int y = threadIdx.x; y < ty; y += blockDim.x) {
+    int32_t acc = 0;
+    for (int x = 0; x < tx; ++x) { acc += gd[y * gw + x]; gd[y * gw + x] = acc; }
+  }
   __syncthreads();
-  for (int v = 0; v < a.V; ++v) {
-    const DevCam c = a.cams[v];
-    const int tx = c.tilesX, ty = c.tilesY, gw = tx + 1;
-    int32_t* gd = a.diffGrid + a.gridBase[v];
-    // rows: prefix along x
-    for (int y = threadIdx.x; y < ty; y += blockDim.x) {
-      int32_t acc = 0;
-      for (int x = 0; x < tx; ++x) { acc += gd[y * gw + x]; gd[y * gw + x] = acc; }
-    }
-    __syncthreads();
-    // columns: prefix along y -> per-tile count
-    uint32_t* cnt = a.tileCnt + c.tileBase;
-    for (int x = threadIdx.x; x < tx; x += blockDim.x) {
-      int32_t acc = 0;
-      for (int y = 0; y < ty; ++y) { acc += gd[y * gw + x]; cnt[y * tx + x] = (uint32_t)acc; }
-    }
-    __syncthreads();
-    // budget: padded prefix; fast path when the whole view fits
-    const int nt = tx * ty;
-    uint64_t local = 0;
-    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
-      const uint32_t cc = cnt[t];
-      uint64_t p = cc;
-      if (cc > SHSORT) { uint64_t q = 1; while (q < cc) q <<= 1; p = q; }
-      local += p;
-    }
-    // block sum of the padded sizes (sums stay far below 2^32 per view in
-    // practice; saturate anyway)
-    uint32_t l32 = local > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)local;
-    uint32_t wsum = __reduce_add_sync(0xFFFFFFFFu, l32);
-    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = wsum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      uint64_t tot = 0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += s_red[w];
-      int drops = 0;
-      uint8_t* dr = a.dropped + c.tileBase;
-      if (tot > a.entriesCap) {
-        // sequential budget rule (shaders.js:357-372)
-        uint64_t acc = 0;
-        for (int t = 0; t < nt; ++t) {
-          const uint32_t cc = cnt[t];
-          uint64_t p = cc;
-          if (cc > SHSORT) { uint64_t q = 1; while (q < cc) q <<= 1; p = q; }
-          if (acc + p > a.entriesCap) { dr[t] = 1; ++drops; }
-          else { dr[t] = 0; acc += p; }
-        }
-      } else {
-        for (int t = 0; t < nt; ++t) dr[t] = 0;
+  // columns: prefix along y -> per-tile count
+  uint32_t* cnt = a.tileCnt + c.tileBase;
+  for (int x = threadIdx.x; x < tx; x += blockDim.x) {
+    int32_t acc = 0;
+    for (int y = 0; y < ty; ++y) { acc += gd[y * gw + x]; cnt[y * tx + x] = (uint32_t)acc; }
+  }
+  __syncthreads();
+  // budget: padded prefix; fast path when the whole view fits
+  const int nt = tx * ty;
+  uint64_t local = 0;
+  for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+    const uint32_t cc = cnt[t];
+    uint64_t p = cc;
+    if (cc > SHSORT) { uint64_t q = 1; while (q < cc) q <<= 1; p = q; }
+    local += p;
+  }
+  const uint32_t l32 = local > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)local;
+  const uint32_t wsum = __reduce_add_sync(0xFFFFFFFFu, l32);
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = wsum;
+  __syncthreads();
+  uint8_t* dr = a.dropped + c.tileBase;
+  if (threadIdx.x == 0) {
+    uint64_t tot = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += s_red[w];
+    int drops = 0;
+    if (tot > a.entriesCap) {
+      // sequential budget rule (shaders.js:357-372)
+      uint64_t acc = 0;
+      for (int t = 0; t < nt; ++t) {
+        const uint32_t cc = cnt[t];
+        uint64_t p = cc;
+        if (cc > SHSORT) { uint64_t q = 1; while (q < cc) q <<= 1; p = q; }
+        if (acc + p > a.entriesCap) { dr[t] = 1; ++drops; }
+        else { dr[t] = 0; acc += p; }
       }
-      a.viewDrops[v] = (uint32_t)drops;
-      if (drops) atomicAdd(&a.stats[3], (uint32_t)drops);
     }
-    __syncthreads();
-    // exclusive scan of kept counts in tile order -> ranges
-    const uint8_t* dr = a.dropped + c.tileBase;
-    const int per = (nt + blockDim.x - 1) / blockDim.x;
-    const int t0 = threadIdx.x * per;
-    uint32_t mine = 0;
-    for (int t = t0; t < min(nt, t0 + per); ++t) mine += dr[t] ? 0u : cnt[t];
-    // block exclusive scan of `mine`
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    uint32_t inc = mine;
+    s_red[32] = (uint32_t)drops;
+    a.viewDrops[v] = (uint32_t)drops;
+    if (drops) atomicAdd(&a.stats[3], (uint32_t)drops);
+  }
+  __syncthreads();
+  const bool anyDrop = s_red[32] != 0;
+  if (!anyDrop)
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) dr[t] = 0;
+  __syncthreads();
+  // exclusive scan of kept counts in tile order -> view-local ranges
+  const int per = (nt + blockDim.x - 1) / blockDim.x;
+  const int t0 = threadIdx.x * per;
+  uint32_t mine = 0;
+  for (int t = t0; t < min(nt, t0 + per); ++t) mine += dr[t] ? 0u : cnt[t];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t inc = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t yv = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+    if (lane >= o) inc += yv;
+  }
+  __syncthreads();
+  if (lane == 31) s_red[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    const uint32_t w = (lane < (int)(blockDim.x >> 5)) ? s_red[lane] : 0u;
+    uint32_t wi = w;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, inc, o);
-      if (lane >= o) inc += y;
+      const uint32_t yv = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+      if (lane >= o) wi += yv;
     }
-    __syncthreads();
-    if (lane == 31) s_red[wid] = inc;
-    __syncthreads();
-    if (wid == 0) {
-      uint32_t w = (lane < (int)(blockDim.x >> 5)) ? s_red[lane] : 0u;
-      uint32_t wi = w;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
-        if (lane >= o) wi += y;
-      }
-      s_red[lane] = wi - w;  // exclusive prefix of warp sums
-    }
-    __syncthreads();
-    uint32_t run = s_base + s_red[wid] + (inc - mine);
-    uint2* rg = a.ranges + c.tileBase;
-    for (int t = t0; t < min(nt, t0 + per); ++t) {
-      const uint32_t k = dr[t] ? 0u : cnt[t];
-      rg[t] = make_uint2(run, run + k);
-      run += k;
-    }
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) s_base = run;
-    __syncthreads();
+    s_red[lane] = wi - w;
+    if (lane == 31) a.viewTotal[v] = wi;
   }
-  if (threadIdx.x == 0) a.totalEntries[0] = s_base;
+  __syncthreads();
+  uint32_t run = s_red[wid] + (inc - mine);
+  uint2* rg = a.ranges + c.tileBase;
+  for (int t = t0; t < min(nt, t0 + per); ++t) {
+    const uint32_t k = dr[t] ? 0u : cnt[t];
+    rg[t] = make_uint2(run, run + k);
+    run += k;
+  }
 }
 
-// Entries each (view, splat) contributes: its bbox area, minus budget-dropped
-// tiles when its view dropped any.
+// Offsets every view's tile ranges by the entries of the views before it and
+// writes the batch's entry total.
+__global__ void k_tile_ranges_finish(TileRangeArgs a, uint32_t totalTiles) {
+  const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gt == 0) {
+    uint32_t tot = 0;
+    for (int v = 0; v < a.V; ++v) tot += a.viewTotal[v];
+    a.totalEntries[0] = tot;
+  }
+  if (gt >= totalTiles) return;
+  int v = 0;
+  while (v + 1 < a.V && a.cams[v + 1].tileBase <= gt) ++v;
+  uint32_t base = 0;
+  for (int u = 0; u < v; ++u) base += a.viewTotal[u];
+  const uint2 r = a.ranges[gt];
+  a.ranges[gt] = make_uint2(r.x + base, r.y + base);
+}
+
+// Entries each presorted item contributes: its bbox area, minus
+// budget-dropped tiles when its view dropped any.
 __global__ void __launch_bounds__(256) k_splat_counts(SplatCountArgs a) {
-  const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= (uint64_t)a.n * a.V) return;
-  const uint32_t v = (uint32_t)(gid / a.n);
-  const uint2 r = a.rect[gid];
+  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= (uint64_t)a.n * a.V) return;
+  const uint32_t slot = a.sortedSlots[p];
+  const uint32_t v = slot / a.n;
+  const uint2 r = a.rect[slot];
   uint32_t cnt = 0;
   if (r.x != 0xFFFFFFFFu) {
     const uint32_t x0 = r.x & 0xFFFFu, y0 = r.x >> 16, x1 = r.y & 0xFFFFu, y1 = r.y >> 16;
@@ -234,31 +260,30 @@ __global__ void __launch_bounds__(256) k_splat_counts(SplatCountArgs a) {
         for (uint32_t x = x0; x <= x1; ++x) cnt += dr[y * c.tilesX + x] ? 0u : 1u;
     }
   }
-  a.counts[gid] = cnt;
+  a.counts[p] = cnt;
 }
 
-// Key generation: entry (globalTile << 32 | depth f32 bits, splat id), written
-// in (view, splat, tile row-major) order so a stable sort by key leaves equal
-// keys in id order -- the reference's (key, id) tie-break (shaders.js:454).
+// Key generation in presorted (view, depth, id) order: one entry per
+// (splat, kept tile), key = global tile id, value = splat id.
 __global__ void __launch_bounds__(256) k_keygen(KeygenArgs a) {
-  const uint64_t gid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= (uint64_t)a.n * a.V) return;
-  const uint2 r = a.rect[gid];
+  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= (uint64_t)a.n * a.V) return;
+  const uint32_t slot = a.sortedSlots[p];
+  const uint2 r = a.rect[slot];
   if (r.x == 0xFFFFFFFFu) return;
-  const uint32_t v = (uint32_t)(gid / a.n);
-  const uint32_t i = (uint32_t)(gid - (uint64_t)v * a.n);
+  const uint32_t v = slot / a.n;
+  const uint32_t i = slot - v * a.n;
   const DevCam& c = a.cams[v];
   const uint32_t x0 = r.x & 0xFFFFu, y0 = r.x >> 16, x1 = r.y & 0xFFFFu, y1 = r.y >> 16;
-  const uint32_t depthBits = __float_as_uint(a.depth[gid]);
   const uint8_t* dr = a.dropped + c.tileBase;
   const bool anyDrop = a.viewDrops[v] != 0;
-  uint32_t o = a.offsets[gid];
+  uint32_t o = a.offsets[p];
   for (uint32_t y = y0; y <= y1; ++y)
     for (uint32_t x = x0; x <= x1; ++x) {
       const uint32_t t = y * c.tilesX + x;
       if (anyDrop && dr[t]) continue;
       if (o < a.capacity) {
-        a.keys[o] = ((uint64_t)(c.tileBase + t) << 32) | depthBits;
+        a.keys[o] = c.tileBase + t;
         a.vals[o] = i;
       } else {
         atomicOr(a.status, ST_ENTRY_OVERFLOW);
@@ -268,8 +293,7 @@ __global__ void __launch_bounds__(256) k_keygen(KeygenArgs a) {
 }
 
 void launch_project(const ProjectArgs& a, int deg, cudaStream_t s) {
-  const uint64_t total = (uint64_t)a.n * a.V;
-  const unsigned grid = (unsigned)((total + 255) / 256);
+  const unsigned grid = (a.n + 255) / 256;
   if (grid == 0) return;
   switch (deg) {
     case 0: k_project<0><<<grid, 256, 0, s>>>(a); break;
@@ -278,7 +302,10 @@ void launch_project(const ProjectArgs& a, int deg, cudaStream_t s) {
     default: k_project<3><<<grid, 256, 0, s>>>(a); break;
   }
 }
-void launch_tile_ranges(const TileRangeArgs& a, cudaStream_t s) { k_tile_ranges<<<1, 1024, 0, s>>>(a); }
+void launch_tile_ranges(const TileRangeArgs& a, uint32_t totalTiles, cudaStream_t s) {
+  k_tile_counts<<<a.V, 1024, 0, s>>>(a);
+  k_tile_ranges_finish<<<(totalTiles + 255) / 256, 256, 0, s>>>(a, totalTiles);
+}
 void launch_splat_counts(const SplatCountArgs& a, cudaStream_t s) {
   const uint64_t total = (uint64_t)a.n * a.V;
   const unsigned grid = (unsigned)((total + 255) / 256);

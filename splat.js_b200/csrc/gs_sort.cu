@@ -140,13 +140,15 @@ constexpr uint32_t FLAG_AGG = 1u, FLAG_INC = 2u;
 constexpr uint32_t LOOKBACK_SPIN_LIMIT = 1u << 22;
 
 // Histogram of every digit position: one read of all keys.
+template <typename KT>
 __global__ void __launch_bounds__(256) k_radix_hist(RadixHistArgs a) {
   __shared__ uint32_t h[RS_MAX_PASSES][256];
   for (int i = threadIdx.x; i < RS_MAX_PASSES * 256; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
   const uint32_t N = *a.nItems;
+  const KT* keys = static_cast<const KT*>(a.keys);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-    const uint64_t k = a.keys[i];
+    const KT k = keys[i];
     for (int p = 0; p < a.passes; ++p) atomicAdd(&h[p][(k >> (8 * p)) & 0xFF], 1u);
   }
   __syncthreads();
@@ -162,10 +164,13 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   return m;
 }
 
+template <typename KT>
 __global__ void __launch_bounds__(RS_THREADS) k_onesweep(OnesweepArgs a) {
   extern __shared__ __align__(16) unsigned char rs_dyn[];
-  uint64_t* s_keys = reinterpret_cast<uint64_t*>(rs_dyn);                  // RS_TILE keys
-  uint32_t* s_vals = reinterpret_cast<uint32_t*>(rs_dyn + RS_TILE * 8);     // RS_TILE values
+  KT* s_keys = reinterpret_cast<KT*>(rs_dyn);                                    // RS_TILE keys
+  uint32_t* s_vals = reinterpret_cast<uint32_t*>(rs_dyn + RS_TILE * sizeof(KT));  // RS_TILE values
+  const KT* keysIn = static_cast<const KT*>(a.keysIn);
+  KT* keysOut = static_cast<KT*>(a.keysOut);
   __shared__ uint32_t s_whist[RS_WARPS][256];
   __shared__ uint32_t s_count[256];     // this block's count per digit
   __shared__ uint32_t s_local[256];     // exclusive prefix of s_count over digits
@@ -213,14 +218,14 @@ __global__ void __launch_bounds__(RS_THREADS) k_onesweep(OnesweepArgs a) {
     const uint32_t base = tile * RS_TILE;
 
     // load: warp w holds entries [base + w*512, +512), item j at lane l
-    uint64_t key[RS_ITEMS];
+    KT key[RS_ITEMS];
     uint32_t val[RS_ITEMS];
     uint32_t dig[RS_ITEMS];
 #pragma unroll
     for (int j = 0; j < RS_ITEMS; ++j) {
       const uint32_t idx = base + wid * (32 * RS_ITEMS) + j * 32 + lane;
       if (idx < N) {
-        key[j] = a.keysIn[idx];
+        key[j] = keysIn[idx];
         val[j] = a.valsIn[idx];
         dig[j] = (uint32_t)(key[j] >> shift) & 0xFFu;
       } else {
@@ -339,39 +344,46 @@ __global__ void __launch_bounds__(RS_THREADS) k_onesweep(OnesweepArgs a) {
     __syncthreads();
     const uint32_t cnt = min((uint32_t)RS_TILE, N - base);
     for (uint32_t i = tid; i < cnt; i += RS_THREADS) {
-      const uint64_t k = s_keys[i];
+      const KT k = s_keys[i];
       const uint32_t d = (uint32_t)(k >> shift) & 0xFFu;
       const uint32_t g = s_gbase[d] + (i - s_local[d]);
-      if (a.keysOut) a.keysOut[g] = k;
+      if (keysOut) keysOut[g] = k;
       a.valsOut[g] = s_vals[i];
     }
     __syncthreads();
   }
 }
 
-constexpr size_t RS_DYN_SMEM = (size_t)RS_TILE * 12;
+template <typename KT>
+constexpr size_t rs_dyn_smem() { return (size_t)RS_TILE * (sizeof(KT) + 4); }
 
 int onesweep_grid(int device) {
-  int sms = 0, perSm = 0;
+  int sms = 0, per32 = 0, per64 = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS_DYN_SMEM);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_onesweep, RS_THREADS, RS_DYN_SMEM);
+  cudaFuncSetAttribute(k_onesweep<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)rs_dyn_smem<uint32_t>());
+  cudaFuncSetAttribute(k_onesweep<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)rs_dyn_smem<uint64_t>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_onesweep<uint32_t>, RS_THREADS, rs_dyn_smem<uint32_t>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per64, k_onesweep<uint64_t>, RS_THREADS, rs_dyn_smem<uint64_t>());
+  int perSm = per32 < per64 ? per32 : per64;  // one grid size that is fully resident for both key widths
   if (perSm < 1) perSm = 1;
   return sms * perSm;
 }
 
-// Sorts N = *nItems entries (N known only on the device) on key bits
-// [0, 8*passes).  Result lands in (keys,vals)[passes & 1 ? 1 : 0] of the
-// ping-pong pair.  hist must hold passes*256 u32, tileCounter passes u32;
-// the caller clears both before the call.
-void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s) {
+// Sorts N = *nItems entries (N known only on the device) with keys of
+// keyBytes (4 or 8) on key bits [0, 8*passes).  Result lands in
+// (keys,vals)[passes & 1] of the ping-pong pair.  hist must hold passes*256
+// u32, tileCounter passes u32; the caller clears both before the call.
+template <typename KT>
+static void radix_sort_t(const RadixSortArgs& a, cudaStream_t s) {
   RadixHistArgs h;
   h.keys = a.keys[0];
   h.nItems = a.nItems;
   h.hist = a.hist;
   h.passes = a.passes;
   h.epoch = a.epoch;
-  k_radix_hist<<<a.histGrid, 256, 0, s>>>(h);
+  k_radix_hist<KT><<<a.histGrid, 256, 0, s>>>(h);
   for (int p = 0; p < a.passes; ++p) {
     OnesweepArgs o;
     o.keysIn = a.keys[p & 1];
@@ -385,8 +397,13 @@ void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s) {
     o.statusWord = a.statusWord;
     o.epoch = a.epoch;
     o.pass = p;
-    k_onesweep<<<a.sweepGrid, RS_THREADS, RS_DYN_SMEM, s>>>(o);
+    k_onesweep<KT><<<a.sweepGrid, RS_THREADS, rs_dyn_smem<KT>(), s>>>(o);
   }
+}
+
+void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s) {
+  if (a.keyBytes == 4) radix_sort_t<uint32_t>(a, s);
+  else radix_sort_t<uint64_t>(a, s);
 }
 
 }  // namespace gs

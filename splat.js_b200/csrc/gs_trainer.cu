@@ -29,6 +29,7 @@ constexpr int RING = 8;      // pinned step-parameter slots
 struct StepParams {
   AdamHP hp;
   uint32_t gridBase[MAXB];
+  uint32_t itemCount;        // V * n presort items of this step
   DevCam cams[MAXB];
 };
 
@@ -74,7 +75,6 @@ struct gs_trainer {
   // ---- device buffers ----
   float *params = nullptr, *m = nullptr, *v = nullptr, *sh = nullptr, *shM = nullptr, *shV = nullptr;
   RenderRec* recs = nullptr;
-  float* depth = nullptr;
   uint2* rect = nullptr;
   uint32_t *counts = nullptr, *offsets = nullptr;
   int32_t* gradP = nullptr;
@@ -84,8 +84,11 @@ struct gs_trainer {
   uint2* ranges = nullptr;
   uint32_t* viewDrops = nullptr;
   uint32_t* workOrder = nullptr;
-  uint64_t* keys[2] = {nullptr, nullptr};
-  uint32_t* vals[2] = {nullptr, nullptr};
+  uint32_t* keys[2] = {nullptr, nullptr};     // entries: global tile id
+  uint32_t* vals[2] = {nullptr, nullptr};     // entries: splat id
+  uint64_t* pkeys[2] = {nullptr, nullptr};    // presort items: view << 32 | depth bits
+  uint32_t* pvals[2] = {nullptr, nullptr};    // presort items: slot = view * n + splat
+  uint32_t* viewTotal = nullptr;
   uint64_t capacity = 0;
   uint32_t* small = nullptr;  // [0,2048) hist | [2048,2056) tileCounter | 2056 workCounter | 2057 totalEntries | 2058 scanTotal | 2059 epoch | 2060 status
   uint64_t* lbStatus = nullptr;
@@ -365,7 +368,11 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   GS_AL(h->shM, std::max<size_t>(shn, 1));
   GS_AL(h->shV, std::max<size_t>(shn, 1));
   GS_AL(h->recs, (size_t)B * cap);
-  GS_AL(h->depth, (size_t)B * cap);
+  GS_AL(h->pkeys[0], (size_t)B * cap);
+  GS_AL(h->pkeys[1], (size_t)B * cap);
+  GS_AL(h->pvals[0], (size_t)B * cap);
+  GS_AL(h->pvals[1], (size_t)B * cap);
+  GS_AL(h->viewTotal, (size_t)MAXB);
   GS_AL(h->rect, (size_t)B * cap);
   GS_AL(h->counts, (size_t)B * cap);
   GS_AL(h->offsets, (size_t)B * cap);
@@ -382,7 +389,7 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   GS_AL(h->vals[0], h->capacity);
   GS_AL(h->vals[1], h->capacity);
   GS_AL(h->small, (size_t)4096);
-  GS_AL(h->lbStatus, (size_t)(h->capacity / 4096 + 2) * 256);
+  GS_AL(h->lbStatus, (size_t)(std::max<uint64_t>(h->capacity, (uint64_t)B * cap) / 4096 + 2) * 256);
   GS_AL(h->scanPartials, (size_t)scan_partials_needed((uint64_t)B * cap) + 1);
   GS_AL(h->outImg, (size_t)B * h->maxPix);
   GS_AL(h->finalT, (size_t)B * h->maxPix);
@@ -411,7 +418,7 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   }
   GS_CK(cudaMemsetAsync(h->gradP, 0, (size_t)B * cap * GP_STRIDE * 4, s));
   GS_CK(cudaMemsetAsync(h->small, 0, 4096 * 4, s));
-  GS_CK(cudaMemsetAsync(h->lbStatus, 0, (size_t)(h->capacity / 4096 + 2) * 256 * 8, s));
+  GS_CK(cudaMemsetAsync(h->lbStatus, 0, (size_t)(std::max<uint64_t>(h->capacity, (uint64_t)B * cap) / 4096 + 2) * 256 * 8, s));
   GS_CK(cudaMemcpyAsync(h->targets, packed.data(), std::max<uint64_t>(total, 4) * 4, cudaMemcpyHostToDevice, s));
   GS_CK(cudaMemsetAsync(h->stats, 0, 16, s));
   GS_CK(cudaMemsetAsync(h->gradCam, 0, (size_t)(ncams + 1) * 32, s));
@@ -498,6 +505,7 @@ static int upload_params(gs_trainer* h, const DevCam* views, int V, const AdamHP
   cudaEventSynchronize(h->ringEv[k]);
   StepParams& P = h->hRing[k];
   P.hp = hp;
+  P.itemCount = (uint32_t)((uint64_t)V * h->n);
   uint32_t tb = 0, pb = 0, gb = 0;
   for (int v = 0; v < V; ++v) {
     P.cams[v] = views[v];
@@ -544,6 +552,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   }
   cudaMemsetAsync(h->diffGrid, 0, (size_t)gridCells * 4, s);
   cudaMemsetAsync(h->small, 0, 2057 * 4, s);  // hist, tile counters, work counter
+  const uint64_t items = (uint64_t)sh.n * V;
 
   ProjectArgs pa{};
   pa.params = h->params;
@@ -556,7 +565,8 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   pa.radClamp = h->o.radClamp;
   pa.tile = sh.tile;
   pa.recs = h->recs;
-  pa.depth = h->depth;
+  pa.pkeys = h->pkeys[0];
+  pa.pvals = h->pvals[0];
   pa.rect = h->rect;
   pa.diffGrid = h->diffGrid;
   pa.gridBase = h->dParams->gridBase;
@@ -571,28 +581,52 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   ta.dropped = h->dropped;
   ta.ranges = h->ranges;
   ta.viewDrops = h->viewDrops;
+  ta.viewTotal = h->viewTotal;
   ta.stats = h->stats;
   ta.entriesCap = h->entriesCap;
   ta.totalEntries = totalEntries;
-  launch_tile_ranges(ta, s);
+  launch_tile_ranges(ta, totalTiles, s);
+
+  // presort of the (view, splat) items by (view, depth): 4 byte digits of
+  // depth, one more for the view index when the batch has several views
+  uint32_t* nItems = h->small + 2061;
+  cudaMemcpyAsync(nItems, &h->dParams->itemCount, 4, cudaMemcpyDeviceToDevice, s);
+  RadixSortArgs pr{};
+  pr.keys[0] = h->pkeys[0]; pr.keys[1] = h->pkeys[1];
+  pr.vals[0] = h->pvals[0]; pr.vals[1] = h->pvals[1];
+  pr.keyBytes = 8;
+  pr.nItems = nItems;
+  pr.hist = hist;
+  pr.tileCounter = tileCounter;
+  pr.status = h->lbStatus;
+  pr.statusWord = statusWord;
+  pr.epoch = epoch;
+  pr.passes = V > 1 ? 5 : 4;
+  pr.keepKeys = false;
+  pr.histGrid = (unsigned)h->histGrid;
+  pr.sweepGrid = (unsigned)h->sweepGrid;
+  if (h->profiling) cudaEventRecord(ph[1], s);
+  launch_radix_sort(pr, s);
+  const uint32_t* sortedSlots = h->pvals[pr.passes & 1];
 
   SplatCountArgs ca{};
   ca.n = sh.n;
   ca.V = V;
   ca.cams = dcams;
+  ca.sortedSlots = sortedSlots;
   ca.rect = h->rect;
   ca.dropped = h->dropped;
   ca.viewDrops = h->viewDrops;
   ca.counts = h->counts;
   launch_splat_counts(ca, s);
-  launch_exclusive_scan(h->counts, (uint64_t)sh.n * V, h->offsets, h->scanPartials, scanTotal, s);
+  launch_exclusive_scan(h->counts, items, h->offsets, h->scanPartials, scanTotal, s);
 
   KeygenArgs ka{};
   ka.n = sh.n;
   ka.V = V;
   ka.cams = dcams;
+  ka.sortedSlots = sortedSlots;
   ka.rect = h->rect;
-  ka.depth = h->depth;
   ka.dropped = h->dropped;
   ka.viewDrops = h->viewDrops;
   ka.offsets = h->offsets;
@@ -602,11 +636,13 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   ka.status = statusWord;
   launch_keygen(ka, s);
 
-  if (h->profiling) cudaEventRecord(ph[1], s);
-  const int passes = (32 + bits_for(totalTiles ? totalTiles - 1 : 0) + 7) / 8;
+  // stable sort of the entries by global tile id
+  cudaMemsetAsync(h->small, 0, 2056 * 4, s);  // histograms and block counters of the second sort
+  const int passes = (bits_for(totalTiles ? totalTiles - 1 : 0) + 7) / 8;
   RadixSortArgs ra{};
   ra.keys[0] = h->keys[0]; ra.keys[1] = h->keys[1];
   ra.vals[0] = h->vals[0]; ra.vals[1] = h->vals[1];
+  ra.keyBytes = 4;
   ra.nItems = totalEntries;
   ra.hist = hist;
   ra.tileCounter = tileCounter;
@@ -1169,7 +1205,7 @@ int gs_refine(gs_trainer* h, gs_rng_fn rng, void* ctx, gs_refine_result* out) {
   launch_exclusive_scan(h->rf.deadFlag, n, h->rf.deadOff, h->rf.partials, h->rf.counts + 0, s);
   launch_exclusive_scan(h->rf.donorFlag, n, h->rf.donorOff, h->rf.partials, h->rf.counts + 1, s);
   launch_refine_compact(h->params, n, h->rf.deadFlag, h->rf.deadOff, h->rf.donorFlag, h->rf.donorOff,
-                        h->rf.deadList, h->rf.donorList, h->keys[0], h->vals[0], s);
+                        h->rf.deadList, h->rf.donorList, h->pkeys[0], h->pvals[0], s);
   uint32_t cnt[2] = {0, 0};
   GS_CK(cudaMemcpyAsync(cnt, h->rf.counts, 8, cudaMemcpyDeviceToHost, s));
   GS_CK(cudaStreamSynchronize(s));
@@ -1180,8 +1216,9 @@ int gs_refine(gs_trainer* h, gs_rng_fn rng, void* ctx, gs_refine_result* out) {
   // stable sort of the donors by mean log-scale, descending (8 byte digits)
   GS_CK(cudaMemsetAsync(h->small, 0, 2057 * 4, s));
   RadixSortArgs ra{};
-  ra.keys[0] = h->keys[0]; ra.keys[1] = h->keys[1];
-  ra.vals[0] = h->vals[0]; ra.vals[1] = h->vals[1];
+  ra.keys[0] = h->pkeys[0]; ra.keys[1] = h->pkeys[1];
+  ra.vals[0] = h->pvals[0]; ra.vals[1] = h->pvals[1];
+  ra.keyBytes = 8;
   ra.nItems = h->rf.counts + 1;
   ra.hist = h->small;
   ra.tileCounter = h->small + 2048;
@@ -1193,7 +1230,7 @@ int gs_refine(gs_trainer* h, gs_rng_fn rng, void* ctx, gs_refine_result* out) {
   ra.histGrid = (unsigned)h->histGrid;
   ra.sweepGrid = (unsigned)h->sweepGrid;
   launch_radix_sort(ra, s);
-  const uint32_t* bigSorted = h->vals[0];  // 8 passes: result back in buffer 0
+  const uint32_t* bigSorted = h->pvals[0];  // 8 passes: result back in buffer 0
   // the host plan: rng() draws in the reference's order
   const uint32_t moveCap = (uint32_t)std::ceil((double)n * 0.05);
   const uint32_t moved = std::min(nDead, moveCap);
