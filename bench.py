@@ -324,6 +324,9 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         batch_ms, batch_vps = timed(step_batched, args.steps, B)
     clocks = clk.summary()
+    st_b = N.GsState()
+    L.gs_get_state(h, C.byref(st_b))
+    batch_launches = int(st_b.lastLaunches)  # kernels one batched step enqueues
     # ---- uneven-resolution batch (config 3) ----
     for k in range(args.warmup):
         step_uneven(k)
@@ -396,18 +399,13 @@ def run_ours(args):
                              "work": f"{FLOP_PER_PAIR} flop per evaluated pixel-entry pair"},
                 "clocks": clocks,
                 "cpu_baseline": cpu}
-        line["gpu_launches"] = launches_per_step(args.batch) * args.steps
+        line["gpu_launches"] = batch_launches * args.steps
+        line["gpu_launches_per_step"] = batch_launches
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
-
-
-def launches_per_step(V):
-    # project, tile ranges, splat counts, 3 scan kernels, keygen, radix histogram,
-    # 6 onesweep passes (1080p, <= 2^16 tiles), work order, raster, chain+Adam
-    return 1 + 1 + 1 + 3 + 1 + 1 + 6 + 1 + 1 + 1
 
 
 def cpu_baseline_line(args, params, sh, cams):

@@ -97,6 +97,7 @@ typedef struct gs_state {
   uint32_t horizon;
   uint32_t lastEntries;   /* kept (tile, splat) entries of the most recent raster */
   uint32_t stepUploadBytes; /* host->device bytes one step copies (view records + Adam parameters) */
+  uint32_t lastLaunches;  /* kernels the most recent step enqueued (graph nodes that are kernels) */
 } gs_state;
 
 /* refine() result (trainer.js:695, 793). early = the donors<16 return. */

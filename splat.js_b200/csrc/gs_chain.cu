@@ -19,10 +19,13 @@ struct CamGrad7 {
 };
 
 // chain for one visible splat in one view; gp = decoded screen-space grads
+// shp: the splat's SH coefficients in global memory (read through the
+// cache).  The SH coefficient gradients are dRGB[c] * Y[k] for k < aK: the
+// gated dRGB, Y and aK are returned instead of the 3K products.
 template <int DEG>
 __device__ __forceinline__ void chainOne(const DevCam& c, const float* P, const Geom& g, float gp[10],
-                                         const float* sh, float anisoReg, float gF[16], float* shG,
-                                         CamGrad7& cg) {
+                                         const float* shp, float anisoReg, float gF[16], float dRGBo[3],
+                                         float Yo[15], int& aKo, CamGrad7& cg) {
   constexpr int K = DEG > 0 ? (DEG + 1) * (DEG + 1) - 1 : 0;
   const float f = c.f, z = g.pc[2], iz = 1.0f / z;
   // conic -> dilated 2D covariance (shaders.js:758-777)
@@ -167,23 +170,23 @@ __device__ __forceinline__ void chainOne(const DevCam& c, const float* P, const 
   // colour: DC sigmoid chain + SH bands (+ position via view dir) (shaders.js:906-947)
   const float sCol[3] = {sigm(P[10]), sigm(P[11]), sigm(P[12])};
   float dRGB[3] = {gp[7], gp[8], gp[9]};
+  aKo = 0;
   if (K > 0) {
     float cp[3];
     camPosWorld(c, cp);
     const float un[3] = {P[0] - cp[0], P[1] - cp[1], P[2] - cp[2]};
     const float ulen = fmaxf(sqrtf(dot3(un, un)), 1e-9f);
     const float vd[3] = {un[0] / ulen, un[1] / ulen, un[2] / ulen};
-    float Y[15], D[15][3];
-    shBasis<DEG>(vd, Y);
-    shBasisGrad<DEG>(vd, D);
+    shBasis<DEG>(vd, Yo);
     const int aK = shActiveK(c, K);
+    aKo = aK;
     float col[3] = {sCol[0], sCol[1], sCol[2]};
 #pragma unroll
     for (int k = 0; k < K; ++k)
       if (k < aK) {
-        col[0] = col[0] + sh[k] * Y[k];
-        col[1] = col[1] + sh[K + k] * Y[k];
-        col[2] = col[2] + sh[2 * K + k] * Y[k];
+        col[0] = col[0] + __ldg(shp + k) * Yo[k];
+        col[1] = col[1] + __ldg(shp + K + k) * Yo[k];
+        col[2] = col[2] + __ldg(shp + 2 * K + k) * Yo[k];
       }
 #pragma unroll
     for (int j = 0; j < 3; ++j) dRGB[j] = dRGB[j] * (col[j] > 0.0f ? 1.0f : 0.0f);
@@ -191,12 +194,11 @@ __device__ __forceinline__ void chainOne(const DevCam& c, const float* P, const 
 #pragma unroll
     for (int k = 0; k < K; ++k)
       if (k < aK) {
-        shG[k] = dRGB[0] * Y[k];
-        shG[K + k] = dRGB[1] * Y[k];
-        shG[2 * K + k] = dRGB[2] * Y[k];
-        const float wk = dRGB[0] * sh[k] + dRGB[1] * sh[K + k] + dRGB[2] * sh[2 * K + k];
+        const float wk = dRGB[0] * __ldg(shp + k) + dRGB[1] * __ldg(shp + K + k) + dRGB[2] * __ldg(shp + 2 * K + k);
+        float D[3];
+        shBasisGradK<DEG>(k, vd, D);
 #pragma unroll
-        for (int j = 0; j < 3; ++j) gv[j] = gv[j] + wk * D[k][j];
+        for (int j = 0; j < 3; ++j) gv[j] = gv[j] + wk * D[j];
       }
     const float vg = dot3(vd, gv);
 #pragma unroll
@@ -205,6 +207,7 @@ __device__ __forceinline__ void chainOne(const DevCam& c, const float* P, const 
 #pragma unroll
   for (int j = 0; j < 3; ++j) gF[10 + j] = dRGB[j] * sCol[j] * (1.0f - sCol[j]);
   gF[13] = gp[6];
+  dRGBo[0] = dRGB[0]; dRGBo[1] = dRGB[1]; dRGBo[2] = dRGB[2];
 }
 
 __device__ __forceinline__ void adamParam(const AdamHP& h, int slot, float& p, float g, float& m, float& v) {
@@ -224,7 +227,9 @@ __device__ __forceinline__ void adamParam(const AdamHP& h, int slot, float& p, f
   p = pn;
 }
 
-template <int DEG>
+// MULTI: several views are summed (accumulators held per splat); a single
+// view needs none.
+template <int DEG, bool MULTI>
 __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
   constexpr int K = DEG > 0 ? (DEG + 1) * (DEG + 1) - 1 : 0;
   constexpr int SHN = 3 * K > 0 ? 3 * K : 1;
@@ -233,13 +238,17 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
   const int lane = threadIdx.x & 31;
 
   float P[16];
-  float sh[SHN];
   float gFa[16];
-  float shA[SHN];
+  float shA[MULTI ? SHN : 1];
+  float dRGB1[3] = {0.0f, 0.0f, 0.0f};  // single view: SH gradient factors
+  float Y1[15];
+  int aK1 = 0;
 #pragma unroll
   for (int k = 0; k < 16; ++k) { P[k] = 0.0f; gFa[k] = 0.0f; }
+  if (MULTI) {
 #pragma unroll
-  for (int k = 0; k < SHN; ++k) { sh[k] = 0.0f; shA[k] = 0.0f; }
+    for (int k = 0; k < SHN; ++k) shA[k] = 0.0f;
+  }
   if (valid) {
     const float4* P4 = reinterpret_cast<const float4*>(a.params + (size_t)i * STRIDE);
 #pragma unroll
@@ -247,21 +256,17 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
       const float4 t = P4[k];
       P[4 * k] = t.x; P[4 * k + 1] = t.y; P[4 * k + 2] = t.z; P[4 * k + 3] = t.w;
     }
-    if (K > 0) {
-      const float* s = a.sh + (size_t)i * 3 * K;
-#pragma unroll
-      for (int k = 0; k < 3 * K; ++k) sh[k] = s[k];
-    }
   }
+  const float* shp = (K > 0 && valid) ? a.sh + (size_t)i * 3 * K : nullptr;
 
   for (int v = 0; v < a.V; ++v) {
     const DevCam& c = a.cams[v];
     float gF[16];
-    float shG[SHN];
 #pragma unroll
     for (int k = 0; k < 16; ++k) gF[k] = 0.0f;
-#pragma unroll
-    for (int k = 0; k < SHN; ++k) shG[k] = 0.0f;
+    float dRGB[3] = {0.0f, 0.0f, 0.0f};
+    float Y[15];
+    int aK = 0;
     CamGrad7 cg = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f};
     if (valid) {
       const size_t slot = (size_t)v * a.n + i;
@@ -283,7 +288,7 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
           const float lmax = cmid + sqrtf(fmaxf(cmid * cmid - (cva * cvc - g.vb * g.vb), 0.0f));
           const float cden = 1.0f + lmax;
           gp[2] = gp[2] * cden; gp[3] = gp[3] * cden; gp[4] = gp[4] * cden;
-          chainOne<DEG>(c, P, g, gp, sh, a.anisoReg, gF, shG, cg);
+          chainOne<DEG>(c, P, g, gp, shp, a.anisoReg, gF, dRGB, Y, aK, cg);
         }
       }
     }
@@ -299,12 +304,28 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
         }
       }
     }
+    // parameter gradients summed in view order from 0 (as the oracle sums)
 #pragma unroll
     for (int k = 0; k < 16; ++k) gFa[k] = gFa[k] + gF[k];
+    if (MULTI) {
 #pragma unroll
-    for (int k = 0; k < SHN; ++k) shA[k] = shA[k] + shG[k];
+      for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch)
+          shA[ch * K + k] = shA[ch * K + k] + (k < aK ? dRGB[ch] * Y[k] : 0.0f);
+    } else {
+      dRGB1[0] = dRGB[0]; dRGB1[1] = dRGB[1]; dRGB1[2] = dRGB[2];
+#pragma unroll
+      for (int k = 0; k < K; ++k) Y1[k] = Y[k];
+      aK1 = aK;
+    }
   }
   if (!valid) return;
+  // SH coefficient gradient of (channel, k)
+  auto shGradOf = [&](int ch, int k) -> float {
+    if (MULTI) return shA[ch * K + k];
+    return 0.0f + (k < aK1 ? dRGB1[ch] * Y1[k] : 0.0f);
+  };
   if (a.gradF) {
     float4* o = reinterpret_cast<float4*>(a.gradF + (size_t)i * STRIDE);
 #pragma unroll
@@ -312,7 +333,9 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
     if (K > 0) {
       float* so = a.shGrad + (size_t)i * 3 * K;
 #pragma unroll
-      for (int k = 0; k < 3 * K; ++k) so[k] = shA[k];
+      for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+        for (int k = 0; k < K; ++k) so[ch * K + k] = shGradOf(ch, k);
     }
   }
   if (!a.doAdam) return;
@@ -325,7 +348,6 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
     m[4 * k] = mm.x; m[4 * k + 1] = mm.y; m[4 * k + 2] = mm.z; m[4 * k + 3] = mm.w;
     vv[4 * k] = vq.x; vv[4 * k + 1] = vq.y; vv[4 * k + 2] = vq.z; vv[4 * k + 3] = vq.w;
   }
-#pragma unroll
   const AdamHP hpv = *a.hp;
 #pragma unroll
   for (int s = 0; s < 16; ++s) adamParam(hpv, s, P[s], gFa[s], m[s], vv[s]);
@@ -337,33 +359,42 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
     V4[k] = make_float4(vv[4 * k], vv[4 * k + 1], vv[4 * k + 2], vv[4 * k + 3]);
   }
   if (K > 0) {
-    float* shp = a.sh + (size_t)i * 3 * K;
+    float* shw = a.sh + (size_t)i * 3 * K;
     float* shm = a.shM + (size_t)i * 3 * K;
     float* shv = a.shV + (size_t)i * 3 * K;
     const AdamHP& h = hpv;
 #pragma unroll
-    for (int k = 0; k < 3 * K; ++k) {
-      float g = shA[k];
-      if (!(fabsf(g) < 1e18f)) g = 0.0f;
-      const float mk = h.b1 * shm[k] + (1.0f - h.b1) * g;
-      const float vk = h.b2 * shv[k] + (1.0f - h.b2) * g * g;
-      shm[k] = mk;
-      shv[k] = vk;
-      const float mh = mk / h.bc1, vh = vk / h.bc2;
-      shp[k] = sh[k] - h.shLr * mh / (sqrtf(vh) + h.eps);
-    }
+    for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const int j = ch * K + k;
+        float g = shGradOf(ch, k);
+        if (!(fabsf(g) < 1e18f)) g = 0.0f;
+        const float mk = h.b1 * shm[j] + (1.0f - h.b1) * g;
+        const float vk = h.b2 * shv[j] + (1.0f - h.b2) * g * g;
+        shm[j] = mk;
+        shv[j] = vk;
+        const float mh = mk / h.bc1, vh = vk / h.bc2;
+        shw[j] = shw[j] - h.shLr * mh / (sqrtf(vh) + h.eps);
+      }
+  }
+}
+
+template <bool MULTI>
+static void launch_chain_t(const ChainArgs& a, int deg, unsigned grid, cudaStream_t s) {
+  switch (deg) {
+    case 0: k_chain_adam<0, MULTI><<<grid, 128, 0, s>>>(a); break;
+    case 1: k_chain_adam<1, MULTI><<<grid, 128, 0, s>>>(a); break;
+    case 2: k_chain_adam<2, MULTI><<<grid, 128, 0, s>>>(a); break;
+    default: k_chain_adam<3, MULTI><<<grid, 128, 0, s>>>(a); break;
   }
 }
 
 void launch_chain_adam(const ChainArgs& a, int deg, cudaStream_t s) {
   const unsigned grid = (a.n + 127) / 128;
   if (grid == 0) return;
-  switch (deg) {
-    case 0: k_chain_adam<0><<<grid, 128, 0, s>>>(a); break;
-    case 1: k_chain_adam<1><<<grid, 128, 0, s>>>(a); break;
-    case 2: k_chain_adam<2><<<grid, 128, 0, s>>>(a); break;
-    default: k_chain_adam<3><<<grid, 128, 0, s>>>(a); break;
-  }
+  if (a.V > 1) launch_chain_t<true>(a, deg, grid, s);
+  else launch_chain_t<false>(a, deg, grid, s);
 }
 
 }  // namespace gs

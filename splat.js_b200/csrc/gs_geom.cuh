@@ -158,4 +158,31 @@ __device__ __forceinline__ void shBasisGrad(const float v[3], float D[15][3]) {
 #undef GS_SET
 }
 
+// dY_k/dv for one coefficient k (the same expressions as shBasisGrad), so a
+// loop over k need not hold the whole gradient table in registers.
+template <int DEG>
+__device__ __forceinline__ void shBasisGradK(int k, const float v[3], float d[3]) {
+  const float x = v[0], y = v[1], z = v[2];
+  const float xx = x * x, yy = y * y, zz = z * z;
+  float C = 0.0f, a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+  switch (k) {
+    case 0: d[0] = 0.0f; d[1] = -GS_C1; d[2] = 0.0f; return;
+    case 1: d[0] = 0.0f; d[1] = 0.0f; d[2] = GS_C1; return;
+    case 2: d[0] = -GS_C1; d[1] = 0.0f; d[2] = 0.0f; return;
+    case 3: C = GS_C2_0; a0 = y; a1 = x; a2 = 0.0f; break;
+    case 4: C = GS_C2_1; a0 = 0.0f; a1 = z; a2 = y; break;
+    case 5: C = GS_C2_2; a0 = -2.0f * x; a1 = -2.0f * y; a2 = 4.0f * z; break;
+    case 6: C = GS_C2_3; a0 = z; a1 = 0.0f; a2 = x; break;
+    case 7: C = GS_C2_4; a0 = 2.0f * x; a1 = -2.0f * y; a2 = 0.0f; break;
+    case 8: C = GS_C3_0; a0 = 6.0f * x * y; a1 = 3.0f * xx - 3.0f * yy; a2 = 0.0f; break;
+    case 9: C = GS_C3_1; a0 = y * z; a1 = x * z; a2 = x * y; break;
+    case 10: C = GS_C3_2; a0 = -2.0f * x * y; a1 = 4.0f * zz - xx - 3.0f * yy; a2 = 8.0f * y * z; break;
+    case 11: C = GS_C3_3; a0 = -6.0f * x * z; a1 = -6.0f * y * z; a2 = 6.0f * zz - 3.0f * xx - 3.0f * yy; break;
+    case 12: C = GS_C3_4; a0 = 4.0f * zz - 3.0f * xx - yy; a1 = -2.0f * x * y; a2 = 8.0f * x * z; break;
+    case 13: C = GS_C3_5; a0 = 2.0f * x * z; a1 = -2.0f * y * z; a2 = xx - yy; break;
+    default: C = GS_C3_6; a0 = 3.0f * xx - yy; a1 = -2.0f * x * y; a2 = 0.0f; break;
+  }
+  d[0] = C * a0; d[1] = C * a1; d[2] = C * a2;
+}
+
 }  // namespace gs

@@ -265,31 +265,87 @@ __global__ void __launch_bounds__(256) k_splat_counts(SplatCountArgs a) {
 
 // Key generation in presorted (view, depth, id) order: one entry per
 // (splat, kept tile), key = global tile id, value = splat id.
+//
+// A warp expands 32 consecutive presorted items together.  Their entries
+// occupy one contiguous output range (the counts' exclusive scan), which the
+// warp fills 32 entries at a time: each lane finds the item owning its entry
+// by a binary search over the items' offsets (shuffles), then the tile from
+// the entry's rank inside the item's rectangle -- coalesced stores, and no
+// lane waits on a large splat.  Items of views that dropped tiles to the
+// entry budget are written by their own lane, skipping the dropped tiles.
 __global__ void __launch_bounds__(256) k_keygen(KeygenArgs a) {
+  const uint64_t items = (uint64_t)a.n * a.V;
   const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= (uint64_t)a.n * a.V) return;
-  const uint32_t slot = a.sortedSlots[p];
-  const uint2 r = a.rect[slot];
-  if (r.x == 0xFFFFFFFFu) return;
-  const uint32_t v = slot / a.n;
-  const uint32_t i = slot - v * a.n;
-  const DevCam& c = a.cams[v];
-  const uint32_t x0 = r.x & 0xFFFFu, y0 = r.x >> 16, x1 = r.y & 0xFFFFu, y1 = r.y >> 16;
-  const uint8_t* dr = a.dropped + c.tileBase;
-  const bool anyDrop = a.viewDrops[v] != 0;
-  uint32_t o = a.offsets[p];
-  for (uint32_t y = y0; y <= y1; ++y)
-    for (uint32_t x = x0; x <= x1; ++x) {
-      const uint32_t t = y * c.tilesX + x;
-      if (anyDrop && dr[t]) continue;
-      if (o < a.capacity) {
-        a.keys[o] = c.tileBase + t;
-        a.vals[o] = i;
+  const int lane = threadIdx.x & 31;
+  const bool valid = p < items;
+  // lanes past the end get an offset above every entry, keeping offsets sorted
+  uint32_t slot = 0, v = 0, i = 0, cnt = 0, off = 0xFFFFFFFFu, tileBase = 0, tilesX = 1, x0 = 0, y0 = 0, w = 1;
+  bool dropView = false;
+  if (valid) {
+    slot = a.sortedSlots[p];
+    const uint2 r = a.rect[slot];
+    off = a.offsets[p];
+    if (r.x != 0xFFFFFFFFu) {
+      v = slot / a.n;
+      i = slot - v * a.n;
+      const DevCam& c = a.cams[v];
+      tileBase = c.tileBase;
+      tilesX = (uint32_t)c.tilesX;
+      x0 = r.x & 0xFFFFu; y0 = r.x >> 16;
+      const uint32_t x1 = r.y & 0xFFFFu, y1 = r.y >> 16;
+      w = x1 - x0 + 1;
+      dropView = a.viewDrops[v] != 0;
+      if (dropView) {
+        // rare: the view dropped tiles; this lane writes its own entries
+        const uint8_t* dr = a.dropped + tileBase;
+        uint32_t o = off;
+        for (uint32_t y = y0; y <= y1; ++y)
+          for (uint32_t x = x0; x <= x1; ++x) {
+            const uint32_t t = y * tilesX + x;
+            if (dr[t]) continue;
+            if (o < a.capacity) { a.keys[o] = tileBase + t; a.vals[o] = i; }
+            else atomicOr(a.status, ST_ENTRY_OVERFLOW);
+            ++o;
+          }
+      } else {
+        cnt = w * (y1 - y0 + 1);
+      }
+    }
+  }
+  // cooperative expansion of the items without drops (cnt = 0 for the rest)
+  const uint32_t ownEnd = off + cnt;
+  const uint32_t rangeLo = __shfl_sync(0xFFFFFFFFu, off, 0);
+  const uint32_t rangeHi = __reduce_max_sync(0xFFFFFFFFu, cnt ? ownEnd : 0u);
+  for (uint32_t base = rangeLo; base < rangeHi; base += 32) {
+    const uint32_t e = base + (uint32_t)lane;
+    // owner: the last lane whose offset <= e among lanes with entries
+    int lo = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+      const uint32_t o = __shfl_sync(0xFFFFFFFFu, off, lo + step);
+      if (lo + step < 32 && o <= e) lo += step;
+    }
+    // lanes with cnt == 0 share their successor's offset; step forward to the
+    // lane that actually holds entry e
+    const uint32_t oc = __shfl_sync(0xFFFFFFFFu, cnt, lo);
+    const uint32_t oo = __shfl_sync(0xFFFFFFFFu, off, lo);
+    const uint32_t ox = __shfl_sync(0xFFFFFFFFu, x0, lo);
+    const uint32_t oy = __shfl_sync(0xFFFFFFFFu, y0, lo);
+    const uint32_t ow = __shfl_sync(0xFFFFFFFFu, w, lo);
+    const uint32_t otb = __shfl_sync(0xFFFFFFFFu, tileBase, lo);
+    const uint32_t otx = __shfl_sync(0xFFFFFFFFu, tilesX, lo);
+    const uint32_t oi = __shfl_sync(0xFFFFFFFFu, i, lo);
+    if (e < rangeHi && e >= oo && e < oo + oc) {
+      const uint32_t k = e - oo;
+      const uint32_t ry = k / ow, rx = k - ry * ow;
+      if (e < a.capacity) {
+        a.keys[e] = otb + (oy + ry) * otx + (ox + rx);
+        a.vals[e] = oi;
       } else {
         atomicOr(a.status, ST_ENTRY_OVERFLOW);
       }
-      ++o;
     }
+  }
 }
 
 void launch_project(const ProjectArgs& a, int deg, cudaStream_t s) {

@@ -113,6 +113,7 @@ struct gs_trainer {
   int lastV = 0;
   DevCam lastCams[MAXB];
   int lastPasses = 0;
+  uint32_t lastLaunches = 0;
   uint32_t lastTotalTiles = 0;
 
   // ---- refine scratch (allocated at the first refine) ----
@@ -459,6 +460,7 @@ int gs_get_state(const gs_trainer* h, gs_state* out) {
   if (h->ready) cudaMemcpy(&le, h->small + 2057, 4, cudaMemcpyDeviceToHost);
   out->lastEntries = le;
   out->stepUploadBytes = (uint32_t)sizeof(StepParams);
+  out->lastLaunches = h->lastLaunches;
   return GS_OK;
 }
 
@@ -655,6 +657,11 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   ra.sweepGrid = (unsigned)h->sweepGrid;
   launch_radix_sort(ra, s);
   h->lastPasses = passes;
+  // kernels: project, tile counts + finish, presort (histogram + passes),
+  // splat counts, 3 scan kernels, keygen, tile sort (histogram + passes),
+  // [work order], raster, [chain+Adam]
+  h->lastLaunches = 3u + 1u + (uint32_t)pr.passes + 1u + 3u + 1u + 1u + (uint32_t)passes +
+                    (h->o.persistent ? 1u : 0u) + 1u + (sh.chain ? 1u : 0u);
   const uint32_t* sortedIds = h->vals[passes & 1];
 
   const bool persistent = h->o.persistent != 0;

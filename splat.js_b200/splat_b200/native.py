@@ -41,7 +41,8 @@ class GsState(C.Structure):
     _fields_ = [("iter", C.c_uint32), ("n", C.c_uint32), ("cap", C.c_uint32), ("shDeg", C.c_uint32),
                 ("shK", C.c_uint32), ("stride", C.c_uint32), ("ncams", C.c_uint32), ("maxTiles", C.c_uint32),
                 ("pixelsSeen", C.c_uint64), ("entriesCap", C.c_uint64), ("horizon", C.c_uint32),
-                ("lastEntries", C.c_uint32), ("stepUploadBytes", C.c_uint32)]
+                ("lastEntries", C.c_uint32), ("stepUploadBytes", C.c_uint32),
+                ("lastLaunches", C.c_uint32)]
 
 
 class GsRefineResult(C.Structure):
