@@ -191,6 +191,20 @@ GS_API int gs_profile_read(gs_trainer* h, double ms[4], uint32_t launches[4]);
  * the peak the raster kernels' roofline is quoted against. */
 GS_API int gs_probe_fp32_peak(int32_t device, double* tflops);
 
+/* ---- allocation-free entry sort (no reference counterpart) ----
+ * Stable LSD radix sort of n (key, value) pairs held in device memory, in
+ * place, on key bits [0, keyBits): the sort that orders the trainer's
+ * (tile id, splat id) entries, run with its scratch in statically sized
+ * device arrays instead of buffers the trainer allocates, so the call
+ * allocates no memory.  n above GS_STATIC_SORT_MAX returns GS_E_LIMIT.
+ * keys/vals: device pointers on the current device; stream may be NULL.
+ * The first call on a device sets the scratch up (symbol lookup and a
+ * synchronous clear), so make it before any stream capture.  The call
+ * returns after the sort has finished (GS_E_DEVICE on a look-back timeout).
+ * The scratch is shared: calls that overlap in time race. */
+#define GS_STATIC_SORT_MAX (1u << 20)
+GS_API int gs_sort_entries_static(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t keyBits, void* stream);
+
 /* ---- raster configuration (no reference counterpart; results do not depend
  * on it: images and gradients are identical for every tile size and depth,
  * only the per-tile entry lists follow the tile size) ----

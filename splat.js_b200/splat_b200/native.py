@@ -37,6 +37,10 @@ class GsImage(C.Structure):
     _fields_ = [("tw", C.c_uint32), ("th", C.c_uint32), ("rgb", C.POINTER(C.c_float))]
 
 
+GS_E_LIMIT = -5
+STATIC_SORT_MAX = 1 << 20  # GS_STATIC_SORT_MAX of include/splat_b200.h
+
+
 class GsState(C.Structure):
     _fields_ = [("iter", C.c_uint32), ("n", C.c_uint32), ("cap", C.c_uint32), ("shDeg", C.c_uint32),
                 ("shK", C.c_uint32), ("stride", C.c_uint32), ("ncams", C.c_uint32), ("maxTiles", C.c_uint32),
@@ -95,6 +99,7 @@ def lib():
         "gs_profile": (C.c_int, [H, C.c_int32]),
         "gs_profile_read": (C.c_int, [H, P(C.c_double), u32p]),
         "gs_probe_fp32_peak": (C.c_int, [C.c_int32, P(C.c_double)]),
+        "gs_sort_entries_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]),
         "gs_autotune": (C.c_int, [H, u32p, C.c_uint32, C.c_int32, i32p, i32p, f32p]),
         "gs_set_raster_config": (C.c_int, [H, C.c_int32, C.c_int32]),
         "gs_raster_pass": (C.c_int, [H, u32p, C.c_uint32, C.c_int32]),

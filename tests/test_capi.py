@@ -61,3 +61,11 @@ def test_create_without_device_fails_cleanly():
     rc = N.lib().gs_create(None, C.byref(h))
     assert rc != 0
     assert b"device" in N.lib().gs_last_error(None)
+
+
+def test_static_sort_rejects_sizes_above_its_limit():
+    """The allocation-free sort refuses n > GS_STATIC_SORT_MAX before any device work."""
+    rc = N.lib().gs_sort_entries_static(None, None, N.STATIC_SORT_MAX + 1, 16, None)
+    assert rc == N.GS_E_LIMIT
+    hdr = open(os.path.join(ROOT, "include", "splat_b200.h")).read()
+    assert "#define GS_STATIC_SORT_MAX (1u << 20)" in hdr
