@@ -68,6 +68,8 @@ typedef struct gs_options {
   int32_t persistent;      /* 1: raster over a persistent (view, tile) work queue, heaviest tiles first */
   int32_t useGraphs;       /* 1: capture each step shape in a CUDA graph and replay it */
   int32_t device;          /* CUDA device ordinal */
+  int32_t tileCull;        /* 1: tile lists keep only entries whose splat can reach a pixel of the tile
+                              (exact ellipse/tile test); images and gradients are identical either way */
 } gs_options;
 
 /* One camera of setup's cams[] (trainer.js:95-99) with the exposure state

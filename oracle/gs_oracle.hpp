@@ -163,6 +163,7 @@ struct Opts {
   int shDeg = 2;            // trainer.js:32
   int tile = 16;            // TILE (shaders.js:32); 16 is the reference's value
   uint64_t entriesCap = 12000000ull;  // ENTCAP (shaders.js:34, trainer.js:48-49)
+  int tileCull = 0;         // B200 library option (no reference counterpart): culled tile lists
 };
 
 // One view: the Cam uniform of shaders.js:140-152 as _camUniform fills it
@@ -435,6 +436,58 @@ inline uint32_t paddedSize(uint32_t c) {  // shaders.js:330-333
 }
 
 template <class T>
+struct Splat2D {  // per-splat values the raster reads (all from proj)
+  T mx, my, cA, cB, cC, w, opa, r, g, b, cnorm;
+};
+template <class T>
+inline Splat2D<T> splat2D(const T* pr) {
+  Splat2D<T> s;
+  s.mx = pr[0]; s.my = pr[1]; s.cA = pr[3]; s.cB = pr[4]; s.cC = pr[5];
+  s.w = pr[7] * pr[6];  // proj[b+7] * proj[b+6] (shaders.js:569, 651)
+  s.opa = pr[7]; s.r = pr[8]; s.g = pr[9]; s.b = pr[10];
+  // cnorm = 1/(1 + lambda_max) of the dilated 2D covariance (shaders.js:674-678)
+  const T cva = pr[12] + T(0.3), cvc = pr[14] + T(0.3);
+  const T cmid = T(0.5) * (cva + cvc);
+  const T lmax = cmid + std::sqrt(std::fmax(cmid * cmid - (cva * cvc - pr[13] * pr[13]), T(0)));
+  s.cnorm = T(1) / (T(1) + lmax);
+  return s;
+}
+
+// Tile cull of the B200 library (no reference counterpart): keeps a (splat,
+// tile) entry only when some pixel centre of the tile can pass the
+// rasteriser's test e <= eCut and w exp(-e) >= aMin.  The exact minimum of
+// e = hA dx^2 + B dx dy + hC dy^2 over the tile's pixel-centre rectangle is
+// taken in double and compared with min(eCut, eA) (eA = log_f(w / aMin)) plus
+// margins for the FP32 evaluation; the library runs the same sequence, so
+// both keep the same entries.  Culled entries contribute to no pixel.
+inline bool tileLive(float mx, float my, float hA, float B, float hC, float eA, float eCut, int tx, int ty,
+                     int tile, int W, int H) {
+  if (!(hA > 0.0f) || !(hC > 0.0f)) return true;
+  const int xe = std::min(tx * tile + tile, W), ye = std::min(ty * tile + tile, H);
+  const double X0 = ((double)(tx * tile) + 0.5) - (double)mx;
+  const double X1 = ((double)(xe - 1) + 0.5) - (double)mx;
+  const double Y0 = ((double)(ty * tile) + 0.5) - (double)my;
+  const double Y1 = ((double)(ye - 1) + 0.5) - (double)my;
+  const double a = hA, b = B, c = hC;
+  double emin = 0.0;
+  if (!(X0 <= 0.0 && X1 >= 0.0 && Y0 <= 0.0 && Y1 >= 0.0)) {
+    emin = 1.0e300;
+    for (double dx : {X0, X1}) {
+      const double dy = std::fmin(std::fmax(-(b * dx) / (2.0 * c), Y0), Y1);
+      emin = std::fmin(emin, (a * dx) * dx + (b * dx) * dy + (c * dy) * dy);
+    }
+    for (double dy : {Y0, Y1}) {
+      const double dx = std::fmin(std::fmax(-(b * dy) / (2.0 * a), X0), X1);
+      emin = std::fmin(emin, (a * dx) * dx + (b * dx) * dy + (c * dy) * dy);
+    }
+  }
+  const double ax = std::fmax(-X0, X1), ay = std::fmax(-Y0, Y1);
+  const double smax = (a * ax) * ax + (std::fabs(b) * ax) * ay + (c * ay) * ay;
+  const double thr = std::fmin((double)eCut, (double)eA + 1.0e-5) + 2.0e-6 * smax + 1.0e-6;
+  return emin <= thr;
+}
+
+template <class T>
 inline Bins binTiles(const Opts& o, const Cam& c, const T* proj, uint32_t n) {
   Bins b;
   const int tx = tilesX(c, o.tile), ty = tilesY(c, o.tile);
@@ -446,10 +499,18 @@ inline Bins binTiles(const Opts& o, const Cam& c, const T* proj, uint32_t n) {
     if (!(pr[11] > T(0))) continue;
     TileRect r = tileRect<T>(c, o.tile, pr[0], pr[1], pr[15]);
     const float depth = (float)pr[2];
+    float cmx = 0, cmy = 0, chA = 0, cB = 0, chC = 0, ceA = 0;
+    if (o.tileCull) {
+      const Splat2D<T> s2 = splat2D<T>(pr);
+      cmx = (float)s2.mx; cmy = (float)s2.my;
+      chA = (float)(T(0.5) * s2.cA); cB = (float)s2.cB; chC = (float)(T(0.5) * s2.cC);
+      ceA = log_f((float)s2.w / o.aMin);
+    }
     for (int y = r.y0; y <= r.y1; ++y)
       for (int x = r.x0; x <= r.x1; ++x) {
+        b.cnt[y * tx + x]++;  // the budget counts every rectangle tile
+        if (o.tileCull && !tileLive(cmx, cmy, chA, cB, chC, ceA, o.eCut, x, y, o.tile, c.W, c.H)) continue;
         lists[y * tx + x].push_back({fbits(depth), i});
-        b.cnt[y * tx + x]++;
       }
   }
   // budgeted scan (shaders.js:357-372): a tile is dropped when its padded
@@ -535,24 +596,6 @@ struct PixelState {
 //        dcomp = (galpha*opa)*G; dlogit = ga*(1-opa); S = fma(c, aT, S)
 // (x*(1/y) stands in for WGSL's x/y, whose accuracy bound is 2.5 ulp.)
 // ---------------------------------------------------------------------------
-template <class T>
-struct Splat2D {  // per-splat values the raster reads (all from proj)
-  T mx, my, cA, cB, cC, w, opa, r, g, b, cnorm;
-};
-template <class T>
-inline Splat2D<T> splat2D(const T* pr) {
-  Splat2D<T> s;
-  s.mx = pr[0]; s.my = pr[1]; s.cA = pr[3]; s.cB = pr[4]; s.cC = pr[5];
-  s.w = pr[7] * pr[6];  // proj[b+7] * proj[b+6] (shaders.js:569, 651)
-  s.opa = pr[7]; s.r = pr[8]; s.g = pr[9]; s.b = pr[10];
-  // cnorm = 1/(1 + lambda_max) of the dilated 2D covariance (shaders.js:674-678)
-  const T cva = pr[12] + T(0.3), cvc = pr[14] + T(0.3);
-  const T cmid = T(0.5) * (cva + cvc);
-  const T lmax = cmid + std::sqrt(std::fmax(cmid * cmid - (cva * cvc - pr[13] * pr[13]), T(0)));
-  s.cnorm = T(1) / (T(1) + lmax);
-  return s;
-}
-
 template <class T>
 inline T pairExponent(const Splat2D<T>& s, T dx, T dy) {
   // e = 0.5 cA dx^2 + cB dx dy + 0.5 cC dy^2 evaluated as

@@ -22,7 +22,7 @@ _LIB = os.path.join(_HERE, "liboracle.so")
 
 class OOpts(C.Structure):
     _fields_ = [("eCut", C.c_float), ("aMin", C.c_float), ("radClamp", C.c_float), ("anisoReg", C.c_float),
-                ("shDeg", C.c_int32), ("tile", C.c_int32), ("entriesCap", C.c_uint64)]
+                ("shDeg", C.c_int32), ("tile", C.c_int32), ("entriesCap", C.c_uint64), ("tileCull", C.c_int32)]
 
 
 class OCam(C.Structure):
@@ -101,8 +101,10 @@ def _p(a, ct):
     return a.ctypes.data_as(C.POINTER(ct))
 
 
-def opts(eCut=4.5, aMin=0.0039, radClamp=1.0, anisoReg=0.005, shDeg=2, tile=16, entriesCap=12_000_000):
-    return OOpts(eCut, aMin, radClamp, anisoReg, shDeg, tile, entriesCap)
+def opts(eCut=4.5, aMin=0.0039, radClamp=1.0, anisoReg=0.005, shDeg=2, tile=16, entriesCap=12_000_000, tileCull=0):
+    """tileCull=1 mirrors the B200 library's culled tile lists (its default);
+    0 keeps the reference's full rectangle lists."""
+    return OOpts(eCut, aMin, radClamp, anisoReg, shDeg, tile, entriesCap, tileCull)
 
 
 def cam(R, t, f, cx, cy, w, h, gain=1.0, bias=0.0, offset=0, camIdx=0, ncams=1, activeSh=2.0, train=1):

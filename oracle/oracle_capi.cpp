@@ -18,6 +18,7 @@ struct OOpts {
   float eCut, aMin, radClamp, anisoReg;
   int32_t shDeg, tile;
   uint64_t entriesCap;
+  int32_t tileCull;
 };
 struct OCam {
   float R[9];
@@ -37,7 +38,7 @@ struct OAdam {
 static Opts toOpts(const OOpts* o) {
   Opts r;
   r.eCut = o->eCut; r.aMin = o->aMin; r.radClamp = o->radClamp; r.anisoReg = o->anisoReg;
-  r.shDeg = o->shDeg; r.tile = o->tile; r.entriesCap = o->entriesCap;
+  r.shDeg = o->shDeg; r.tile = o->tile; r.entriesCap = o->entriesCap; r.tileCull = o->tileCull;
   return r;
 }
 static Cam toCam(const OCam* c) {

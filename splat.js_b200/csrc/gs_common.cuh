@@ -89,6 +89,50 @@ __device__ __forceinline__ float glog(float x) {
   return __fmaf_rn(fe, 0.693145751953125f, __fmaf_rn(fe, 1.42860676533018700e-6f, lm));
 }
 
+// Tile cull: can any pixel centre of tile (tx, ty) pass the rasteriser's
+// test (e <= eCut and alpha = w exp(-e) >= aMin) for the splat with mean
+// (mx, my) and conic halves (hA, B, hC)?  The exact minimum of
+// e = hA dx^2 + B dx dy + hC dy^2 over the rectangle of the tile's pixel
+// centres (clipped to the image) is computed in double and compared with
+// min(eCut, ln(w / aMin)) plus margins that cover the rasteriser's FP32
+// evaluation (a few ulp of the largest term, bounded by smax) and the
+// canonical log.  Every pixel that passes the FP32 test lies in a tile that
+// passes this one, so dropping the other entries changes no pixel.  The same
+// double-precision sequence runs in the oracle; results are identical.
+//   eA = glog(w / aMin), computed once per splat.
+__device__ __forceinline__ bool tileLive(float mx, float my, float hA, float B, float hC, float eA, float eCut,
+                                         int tx, int ty, int tile, int W, int H) {
+  if (!(hA > 0.0f) || !(hC > 0.0f)) return true;
+  const int xe = tx * tile + tile < W ? tx * tile + tile : W;
+  const int ye = ty * tile + tile < H ? ty * tile + tile : H;
+  const double X0 = ((double)(tx * tile) + 0.5) - (double)mx;
+  const double X1 = ((double)(xe - 1) + 0.5) - (double)mx;
+  const double Y0 = ((double)(ty * tile) + 0.5) - (double)my;
+  const double Y1 = ((double)(ye - 1) + 0.5) - (double)my;
+  const double a = (double)hA, b = (double)B, c = (double)hC;
+  double emin = 0.0;
+  if (!(X0 <= 0.0 && X1 >= 0.0 && Y0 <= 0.0 && Y1 >= 0.0)) {
+    emin = 1.0e300;
+    const double xs[2] = {X0, X1}, ys[2] = {Y0, Y1};
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const double dx = xs[k];
+      const double dy = fmin(fmax(-(b * dx) / (2.0 * c), Y0), Y1);
+      emin = fmin(emin, (a * dx) * dx + (b * dx) * dy + (c * dy) * dy);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const double dy = ys[k];
+      const double dx = fmin(fmax(-(b * dy) / (2.0 * a), X0), X1);
+      emin = fmin(emin, (a * dx) * dx + (b * dx) * dy + (c * dy) * dy);
+    }
+  }
+  const double ax = fmax(-X0, X1), ay = fmax(-Y0, Y1);
+  const double smax = (a * ax) * ax + (fabs(b) * ax) * ay + (c * ay) * ay;
+  const double thr = fmin((double)eCut, (double)eA + 1.0e-5) + 2.0e-6 * smax + 1.0e-6;
+  return emin <= thr;
+}
+
 // sin(x) in double, |x| < 2^31: quadrant reduction by pi/2 (28-bit head so
 // k * head is exact, plus a tail), Taylor series of sin/cos on |r| <= pi/4.
 __device__ __forceinline__ double gsin_d(double x) {

@@ -39,28 +39,23 @@ struct TileRangeArgs {
   uint32_t* totalEntries;  // out: kept entries over the batch
 };
 
-struct SplatCountArgs {
+// Entry expansion of the presorted (view, depth, id) items (k_expand).
+struct ExpandArgs {
   uint32_t n;
   int V;
   const DevCam* cams;
   const uint32_t* sortedSlots;  // presorted (view, depth, id) order
   const uint2* rect;
+  const RenderRec* recs;        // read when cull != 0
   const uint8_t* dropped;
   const uint32_t* viewDrops;
-  uint32_t* counts;        // V * n, in presorted order
-};
-
-struct KeygenArgs {
-  uint32_t n;
-  int V;
-  const DevCam* cams;
-  const uint32_t* sortedSlots;
-  const uint2* rect;
-  const uint8_t* dropped;
-  const uint32_t* viewDrops;
-  const uint32_t* offsets;  // V * n exclusive scan of counts (presorted order)
-  uint32_t* keys;           // global tile id per entry
-  uint32_t* vals;           // splat id per entry
+  float eCut, aMin;
+  int tile;
+  int cull;                     // 1: keep only entries tileLive() accepts
+  uint32_t* counts;             // count pass: V * n, in presorted order
+  const uint32_t* offsets;      // key pass: V * n exclusive scan of counts
+  uint32_t* keys;               // global tile id per entry
+  uint32_t* vals;               // splat id per entry
   uint64_t capacity;
   uint32_t* status;
 };
@@ -176,8 +171,9 @@ struct RefineApplyArgs {
 // launchers
 void launch_project(const ProjectArgs& a, int deg, cudaStream_t s);
 void launch_tile_ranges(const TileRangeArgs& a, uint32_t totalTiles, cudaStream_t s);
-void launch_splat_counts(const SplatCountArgs& a, cudaStream_t s);
-void launch_keygen(const KeygenArgs& a, cudaStream_t s);
+void launch_expand(const ExpandArgs& a, bool keys, cudaStream_t s);
+void launch_ranges_from_keys(const uint32_t* keys, const uint32_t* nItems, uint32_t totalTiles, uint2* ranges,
+                             cudaStream_t s);
 uint32_t scan_partials_needed(uint64_t N);
 void launch_exclusive_scan(const uint32_t* in, uint64_t N, uint32_t* out, uint32_t* partials, uint32_t* total,
                            cudaStream_t s);

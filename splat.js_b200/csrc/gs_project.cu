@@ -240,112 +240,146 @@ __global__ void k_tile_ranges_finish(TileRangeArgs a, uint32_t totalTiles) {
   a.ranges[gt] = make_uint2(r.x + base, r.y + base);
 }
 
-// Entries each presorted item contributes: its bbox area, minus
-// budget-dropped tiles when its view dropped any.
-__global__ void __launch_bounds__(256) k_splat_counts(SplatCountArgs a) {
-  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= (uint64_t)a.n * a.V) return;
-  const uint32_t slot = a.sortedSlots[p];
-  const uint32_t v = slot / a.n;
-  const uint2 r = a.rect[slot];
-  uint32_t cnt = 0;
-  if (r.x != 0xFFFFFFFFu) {
-    const uint32_t x0 = r.x & 0xFFFFu, y0 = r.x >> 16, x1 = r.y & 0xFFFFu, y1 = r.y >> 16;
-    if (a.viewDrops[v] == 0) {
-      cnt = (x1 - x0 + 1) * (y1 - y0 + 1);
-    } else {
-      const DevCam& c = a.cams[v];
-      const uint8_t* dr = a.dropped + c.tileBase;
-      for (uint32_t y = y0; y <= y1; ++y)
-        for (uint32_t x = x0; x <= x1; ++x) cnt += dr[y * c.tilesX + x] ? 0u : 1u;
-    }
-  }
-  a.counts[p] = cnt;
-}
-
-// Key generation in presorted (view, depth, id) order: one entry per
-// (splat, kept tile), key = global tile id, value = splat id.
+// Entry expansion of the presorted items, in two passes over the same walk:
+// KEYS = false counts each item's entries, KEYS = true writes them at the
+// counts' exclusive scan -- key = global tile id, value = splat id, tiles of
+// an item in row order.  An entry is a tile of the item's rectangle that the
+// entry budget kept and, with culling on, that tileLive() accepts.
 //
-// A warp expands 32 consecutive presorted items together.  Their entries
-// occupy one contiguous output range (the counts' exclusive scan), which the
-// warp fills 32 entries at a time: each lane finds the item owning its entry
-// by a binary search over the items' offsets (shuffles), then the tile from
-// the entry's rank inside the item's rectangle -- coalesced stores, and no
-// lane waits on a large splat.  Items of views that dropped tiles to the
-// entry budget are written by their own lane, skipping the dropped tiles.
-__global__ void __launch_bounds__(256) k_keygen(KeygenArgs a) {
+// A warp walks the candidate (item, tile) pairs of its 32 items 32 at a time:
+// each lane finds the item owning its candidate by a binary search over the
+// items' candidate offsets (shuffles), tests the tile, and a ballot ranks the
+// accepted candidates of each item; so stores are coalesced and no lane waits
+// on a large splat.  Items of views that dropped tiles to the budget are
+// walked by their own lane (rare).
+template <bool KEYS>
+__global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
+  __shared__ uint32_t s_run[256];  // entries of each item so far
   const uint64_t items = (uint64_t)a.n * a.V;
   const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
+  const int wbase = threadIdx.x & ~31;
+  const uint32_t FULL = 0xFFFFFFFFu;
   const bool valid = p < items;
-  // lanes past the end get an offset above every entry, keeping offsets sorted
-  uint32_t slot = 0, v = 0, i = 0, cnt = 0, off = 0xFFFFFFFFu, tileBase = 0, tilesX = 1, x0 = 0, y0 = 0, w = 1;
-  bool dropView = false;
+  uint32_t v = 0, i = 0, x0 = 0, y0 = 0, rw = 1, rc = 0, out = 0;
+  float mx = 0.0f, my = 0.0f, hA = 0.0f, B = 0.0f, hC = 0.0f, eA = 0.0f;
+  s_run[threadIdx.x] = 0;
   if (valid) {
-    slot = a.sortedSlots[p];
+    const uint32_t slot = a.sortedSlots[p];
     const uint2 r = a.rect[slot];
-    off = a.offsets[p];
+    if (KEYS) out = a.offsets[p];
     if (r.x != 0xFFFFFFFFu) {
       v = slot / a.n;
       i = slot - v * a.n;
-      const DevCam& c = a.cams[v];
-      tileBase = c.tileBase;
-      tilesX = (uint32_t)c.tilesX;
       x0 = r.x & 0xFFFFu; y0 = r.x >> 16;
       const uint32_t x1 = r.y & 0xFFFFu, y1 = r.y >> 16;
-      w = x1 - x0 + 1;
-      dropView = a.viewDrops[v] != 0;
-      if (dropView) {
-        // rare: the view dropped tiles; this lane writes its own entries
-        const uint8_t* dr = a.dropped + tileBase;
-        uint32_t o = off;
+      rw = x1 - x0 + 1;
+      if (a.cull) {
+        const float4 q0 = a.recs[slot].r0, q1 = a.recs[slot].r1;
+        mx = q0.x; my = q0.y; hA = q0.z; B = q0.w; hC = q1.x;
+        eA = glog(q1.y / a.aMin);
+      }
+      if (a.viewDrops[v] == 0) {
+        rc = rw * (y1 - y0 + 1);
+      } else {
+        const DevCam& c = a.cams[v];
+        const uint8_t* dr = a.dropped + c.tileBase;
+        uint32_t o = out, cnt = 0;
         for (uint32_t y = y0; y <= y1; ++y)
           for (uint32_t x = x0; x <= x1; ++x) {
-            const uint32_t t = y * tilesX + x;
+            const uint32_t t = y * c.tilesX + x;
             if (dr[t]) continue;
-            if (o < a.capacity) { a.keys[o] = tileBase + t; a.vals[o] = i; }
-            else atomicOr(a.status, ST_ENTRY_OVERFLOW);
-            ++o;
+            if (a.cull && !tileLive(mx, my, hA, B, hC, eA, a.eCut, (int)x, (int)y, a.tile, c.W, c.H)) continue;
+            if (KEYS) {
+              if (o < a.capacity) { a.keys[o] = c.tileBase + t; a.vals[o] = i; }
+              else atomicOr(a.status, ST_ENTRY_OVERFLOW);
+              ++o;
+            }
+            ++cnt;
           }
-      } else {
-        cnt = w * (y1 - y0 + 1);
+        s_run[threadIdx.x] = cnt;
       }
     }
   }
-  // cooperative expansion of the items without drops (cnt = 0 for the rest)
-  const uint32_t ownEnd = off + cnt;
-  const uint32_t rangeLo = __shfl_sync(0xFFFFFFFFu, off, 0);
-  const uint32_t rangeHi = __reduce_max_sync(0xFFFFFFFFu, cnt ? ownEnd : 0u);
-  for (uint32_t base = rangeLo; base < rangeHi; base += 32) {
+  __syncwarp();
+  // candidate offsets of the warp's items (inclusive scan of rc)
+  uint32_t cEnd = rc;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(FULL, cEnd, o);
+    if (lane >= o) cEnd += y;
+  }
+  const uint32_t cBase = cEnd - rc;
+  const uint32_t C = __shfl_sync(FULL, cEnd, 31);
+  const uint32_t ltm = (1u << lane) - 1u;
+  for (uint32_t base = 0; base < C; base += 32) {
     const uint32_t e = base + (uint32_t)lane;
-    // owner: the last lane whose offset <= e among lanes with entries
+    const bool inRange = e < C;
+    // owner: the last lane whose candidate offset is <= e; lanes without
+    // candidates share their successor's offset, so the last one holds e
     int lo = 0;
 #pragma unroll
     for (int step = 16; step >= 1; step >>= 1) {
-      const uint32_t o = __shfl_sync(0xFFFFFFFFu, off, lo + step);
-      if (lo + step < 32 && o <= e) lo += step;
+      const uint32_t ob = __shfl_sync(FULL, cBase, (lo + step) & 31);
+      if (lo + step < 32 && ob <= e) lo += step;
     }
-    // lanes with cnt == 0 share their successor's offset; step forward to the
-    // lane that actually holds entry e
-    const uint32_t oc = __shfl_sync(0xFFFFFFFFu, cnt, lo);
-    const uint32_t oo = __shfl_sync(0xFFFFFFFFu, off, lo);
-    const uint32_t ox = __shfl_sync(0xFFFFFFFFu, x0, lo);
-    const uint32_t oy = __shfl_sync(0xFFFFFFFFu, y0, lo);
-    const uint32_t ow = __shfl_sync(0xFFFFFFFFu, w, lo);
-    const uint32_t otb = __shfl_sync(0xFFFFFFFFu, tileBase, lo);
-    const uint32_t otx = __shfl_sync(0xFFFFFFFFu, tilesX, lo);
-    const uint32_t oi = __shfl_sync(0xFFFFFFFFu, i, lo);
-    if (e < rangeHi && e >= oo && e < oo + oc) {
-      const uint32_t k = e - oo;
-      const uint32_t ry = k / ow, rx = k - ry * ow;
-      if (e < a.capacity) {
-        a.keys[e] = otb + (oy + ry) * otx + (ox + rx);
-        a.vals[e] = oi;
-      } else {
-        atomicOr(a.status, ST_ENTRY_OVERFLOW);
-      }
+    const uint32_t ocb = __shfl_sync(FULL, cBase, lo);
+    const uint32_t ox = __shfl_sync(FULL, x0, lo);
+    const uint32_t oy = __shfl_sync(FULL, y0, lo);
+    const uint32_t orw = __shfl_sync(FULL, rw, lo);
+    const uint32_t ov = __shfl_sync(FULL, v, lo);
+    const uint32_t oi = __shfl_sync(FULL, i, lo);
+    const uint32_t oout = __shfl_sync(FULL, out, lo);
+    const float omx = __shfl_sync(FULL, mx, lo);
+    const float omy = __shfl_sync(FULL, my, lo);
+    const float ohA = __shfl_sync(FULL, hA, lo);
+    const float oB = __shfl_sync(FULL, B, lo);
+    const float ohC = __shfl_sync(FULL, hC, lo);
+    const float oeA = __shfl_sync(FULL, eA, lo);
+    bool live = false;
+    uint32_t gt = 0;
+    if (inRange) {
+      const uint32_t k = e - ocb;
+      const uint32_t ry = k / orw, rx = k - ry * orw;
+      const uint32_t tx = ox + rx, ty = oy + ry;
+      const DevCam& c = a.cams[ov];
+      gt = c.tileBase + ty * (uint32_t)c.tilesX + tx;
+      live = !a.cull || tileLive(omx, omy, ohA, oB, ohC, oeA, a.eCut, (int)tx, (int)ty, a.tile, c.W, c.H);
     }
+    const uint32_t lb = __ballot_sync(FULL, live);
+    const uint32_t peers = __match_any_sync(FULL, inRange ? (uint32_t)lo : 32u);
+    const uint32_t prior = s_run[wbase + lo];
+    if (KEYS && live) {
+      const uint32_t o = oout + prior + __popc(lb & peers & ltm);
+      if (o < a.capacity) { a.keys[o] = gt; a.vals[o] = oi; }
+      else atomicOr(a.status, ST_ENTRY_OVERFLOW);
+    }
+    __syncwarp();
+    if (inRange && lane == __ffs(peers) - 1) s_run[wbase + lo] = prior + __popc(lb & peers);
+    __syncwarp();
   }
+  if (!KEYS && valid) a.counts[p] = s_run[threadIdx.x];
+}
+
+// Per-tile ranges from the sorted entry keys (culled lists): tile gt spans
+// [lower_bound(gt), lower_bound(gt + 1)), so empty and dropped tiles get an
+// empty range at their place in the order, as the budgeted scan gives them.
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* keys, uint32_t E, uint32_t x) {
+  uint32_t lo = 0, hi = E;
+  while (lo < hi) {
+    const uint32_t mid = lo + ((hi - lo) >> 1);
+    if (keys[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(256) k_ranges_from_keys(const uint32_t* keys, const uint32_t* nItems,
+                                                          uint32_t totalTiles, uint2* ranges) {
+  const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gt >= totalTiles) return;
+  const uint32_t E = *nItems;
+  ranges[gt] = make_uint2(lower_bound_u32(keys, E, gt), lower_bound_u32(keys, E, gt + 1));
 }
 
 void launch_project(const ProjectArgs& a, int deg, cudaStream_t s) {
@@ -362,15 +396,16 @@ void launch_tile_ranges(const TileRangeArgs& a, uint32_t totalTiles, cudaStream_
   k_tile_counts<<<a.V, 1024, 0, s>>>(a);
   k_tile_ranges_finish<<<(totalTiles + 255) / 256, 256, 0, s>>>(a, totalTiles);
 }
-void launch_splat_counts(const SplatCountArgs& a, cudaStream_t s) {
+void launch_expand(const ExpandArgs& a, bool keys, cudaStream_t s) {
   const uint64_t total = (uint64_t)a.n * a.V;
   const unsigned grid = (unsigned)((total + 255) / 256);
-  if (grid) k_splat_counts<<<grid, 256, 0, s>>>(a);
+  if (!grid) return;
+  if (keys) k_expand<true><<<grid, 256, 0, s>>>(a);
+  else k_expand<false><<<grid, 256, 0, s>>>(a);
 }
-void launch_keygen(const KeygenArgs& a, cudaStream_t s) {
-  const uint64_t total = (uint64_t)a.n * a.V;
-  const unsigned grid = (unsigned)((total + 255) / 256);
-  if (grid) k_keygen<<<grid, 256, 0, s>>>(a);
+void launch_ranges_from_keys(const uint32_t* keys, const uint32_t* nItems, uint32_t totalTiles, uint2* ranges,
+                             cudaStream_t s) {
+  if (totalTiles) k_ranges_from_keys<<<(totalTiles + 255) / 256, 256, 0, s>>>(keys, nItems, totalTiles, ranges);
 }
 
 }  // namespace gs

@@ -230,6 +230,7 @@ int gs_default_options(gs_options* o) {
   o->persistent = 1;
   o->useGraphs = 1;
   o->device = 0;
+  o->tileCull = 1;
   return GS_OK;
 }
 
@@ -244,6 +245,7 @@ int gs_create(const gs_options* opts, gs_trainer** out) {
   // exp(-e) is evaluated for e <= eCut; the canonical exp is defined on |x| <= 87
   if (!(o.eCut > 0.0f && o.eCut <= 80.0f)) { g_createError = "eCut must be in (0, 80]"; return GS_E_INVALID; }
   if (o.tile != 8 && o.tile != 16 && o.tile != 32) { g_createError = "tile must be 8, 16 or 32"; return GS_E_INVALID; }
+  if (o.tileCull != 0 && o.tileCull != 1) { g_createError = "tileCull must be 0 or 1"; return GS_E_INVALID; }
   if (o.batchDepth != 64 && o.batchDepth != 128 && o.batchDepth != 256) {
     g_createError = "batchDepth must be 64, 128 or 256";
     return GS_E_INVALID;
@@ -611,32 +613,31 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   launch_radix_sort(pr, s);
   const uint32_t* sortedSlots = h->pvals[pr.passes & 1];
 
-  SplatCountArgs ca{};
-  ca.n = sh.n;
-  ca.V = V;
-  ca.cams = dcams;
-  ca.sortedSlots = sortedSlots;
-  ca.rect = h->rect;
-  ca.dropped = h->dropped;
-  ca.viewDrops = h->viewDrops;
-  ca.counts = h->counts;
-  launch_splat_counts(ca, s);
+  const bool cull = h->o.tileCull != 0;
+  ExpandArgs ea{};
+  ea.n = sh.n;
+  ea.V = V;
+  ea.cams = dcams;
+  ea.sortedSlots = sortedSlots;
+  ea.rect = h->rect;
+  ea.recs = h->recs;
+  ea.dropped = h->dropped;
+  ea.viewDrops = h->viewDrops;
+  ea.eCut = h->o.eCut;
+  ea.aMin = h->o.aMin;
+  ea.tile = sh.tile;
+  ea.cull = cull ? 1 : 0;
+  ea.counts = h->counts;
+  ea.offsets = h->offsets;
+  ea.keys = h->keys[0];
+  ea.vals = h->vals[0];
+  ea.capacity = h->capacity;
+  ea.status = statusWord;
+  launch_expand(ea, false, s);
   launch_exclusive_scan(h->counts, items, h->offsets, h->scanPartials, scanTotal, s);
-
-  KeygenArgs ka{};
-  ka.n = sh.n;
-  ka.V = V;
-  ka.cams = dcams;
-  ka.sortedSlots = sortedSlots;
-  ka.rect = h->rect;
-  ka.dropped = h->dropped;
-  ka.viewDrops = h->viewDrops;
-  ka.offsets = h->offsets;
-  ka.keys = h->keys[0];
-  ka.vals = h->vals[0];
-  ka.capacity = h->capacity;
-  ka.status = statusWord;
-  launch_keygen(ka, s);
+  launch_expand(ea, true, s);
+  // culled lists: the entry total is the counts' sum, not the budgeted tile sum
+  if (cull) cudaMemcpyAsync(totalEntries, scanTotal, 4, cudaMemcpyDeviceToDevice, s);
 
   // stable sort of the entries by global tile id
   cudaMemsetAsync(h->small, 0, 2056 * 4, s);  // histograms and block counters of the second sort
@@ -652,15 +653,16 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   ra.statusWord = statusWord;
   ra.epoch = epoch;
   ra.passes = passes;
-  ra.keepKeys = false;
+  ra.keepKeys = cull;  // culled lists take their tile ranges from the sorted keys
   ra.histGrid = (unsigned)h->histGrid;
   ra.sweepGrid = (unsigned)h->sweepGrid;
   launch_radix_sort(ra, s);
   h->lastPasses = passes;
+  if (cull) launch_ranges_from_keys(h->keys[passes & 1], totalEntries, totalTiles, h->ranges, s);
   // kernels: project, tile counts + finish, presort (histogram + passes),
-  // splat counts, 3 scan kernels, keygen, tile sort (histogram + passes),
-  // [work order], raster, [chain+Adam]
-  h->lastLaunches = 3u + 1u + (uint32_t)pr.passes + 1u + 3u + 1u + 1u + (uint32_t)passes +
+  // entry counts, 3 scan kernels, entry keys, tile sort (histogram +
+  // passes), [ranges from keys], [work order], raster, [chain+Adam]
+  h->lastLaunches = 3u + 1u + (uint32_t)pr.passes + 1u + 3u + 1u + 1u + (uint32_t)passes + (cull ? 1u : 0u) +
                     (h->o.persistent ? 1u : 0u) + 1u + (sh.chain ? 1u : 0u);
   const uint32_t* sortedIds = h->vals[passes & 1];
 

@@ -42,11 +42,11 @@ def test_default_options_match_reference():
     assert o.shDeg == 2 and o.tileGrad == 1 and o.capMult == 4.0 and o.maxIters == 60000
     assert o.minScale == pytest.approx(1e-4) and o.opacityReg == pytest.approx(0.01)
     assert o.shLr == pytest.approx(1.25e-4) and o.growRate == pytest.approx(0.15)
-    assert o.tile == 16
+    assert o.tile == 16 and o.tileCull == 1
 
 
 def test_struct_sizes_match_header():
-    assert C.sizeof(N.GsOptions) == 4 * 6 + 8 + 4 * 2 + 8 * 4 + 4 * 2 + 4 * 7 + 4
+    assert C.sizeof(N.GsOptions) == 4 * 6 + 8 + 4 * 2 + 8 * 4 + 4 * 2 + 4 * 8
     assert C.sizeof(N.GsCamera) == 4 * (9 + 3 + 3 + 3) + 8 * 2
     assert C.sizeof(N.GsImage) == 16
     assert C.sizeof(N.GsRefineResult) == 24

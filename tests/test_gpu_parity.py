@@ -41,7 +41,8 @@ def make(params, sh, cams, rgbs, opts, radius=1.5, maxW=None, maxH=None):
 def oracle_opts(opts):
     return O.opts(eCut=opts.get("eCut", 4.5), aMin=opts.get("aMin", 0.0039), radClamp=opts.get("radClamp", 1.0),
                   anisoReg=opts.get("anisoReg", 0.005), shDeg=opts.get("shDeg", 2),
-                  entriesCap=opts.get("entriesCap", 12_000_000), tile=opts.get("tile", 16))
+                  entriesCap=opts.get("entriesCap", 12_000_000), tile=opts.get("tile", 16),
+                  tileCull=opts.get("tileCull", 1))
 
 
 def gpu_raster(t, cis, mode=3):
@@ -167,12 +168,15 @@ def oracle_adam(t, iter_after, radius, horizon=60000, opacityReg=0.01, shLr=1.25
                      float(np.float32(math.log(radius * 0.05))), reg=opacityReg, shLr=shLr)
 
 
-def test_config0_raster_bitexact():
+@pytest.mark.parametrize("cull", [1, 0])
+def test_config0_raster_bitexact(cull):
+    """cull=0: the reference's full rectangle lists, per-tile order included."""
     params, sh, cams, rgbs = config0()
     n = len(params) // 16
-    t, targets, metas = make(params, sh, cams, rgbs, dict(shDeg=2), radius=1.0)
+    opts = dict(shDeg=2, tileCull=cull)
+    t, targets, metas = make(params, sh, cams, rgbs, opts, radius=1.0)
     gpu_raster(t, [0], 3)
-    check_view_against_oracle(t, oracle_opts(dict(shDeg=2)), oracle_cam(metas[0], 0, 1, 2), params, sh, targets, n)
+    check_view_against_oracle(t, oracle_opts(opts), oracle_cam(metas[0], 0, 1, 2), params, sh, targets, n)
 
 
 @pytest.mark.parametrize("steps", [3])
@@ -385,3 +389,33 @@ def test_autotune_picks_a_config_and_keeps_results():
     g1, s1, st1 = t.gradPass(0)
     assert_bits(g1, g0, "gradF after autotune")
     assert_bits(st1, st0, "stats after autotune")
+
+
+def test_tile_cull_changes_no_training_result():
+    """Three batched steps with culled and with full tile lists: parameters,
+    moments and loss statistics bit-identical; fewer entries when culled."""
+    from test_tile_cull import anisotropic_scene
+    n = 4000
+    params, cam = anisotropic_scene(n, 11)
+    sh = np.zeros(n * 3 * 8, np.float32)
+    p0, s0, cams0, rgbs0 = config0(n=3000, seed=2)
+    cams = [cam, dict(cams0[0])]
+    rgbs = [scene.uniform_target(256, 256, seed=11), rgbs0[0]]
+    res = {}
+    for cull in (0, 1):
+        t, targets, metas = make(params, sh, [dict(c) for c in cams], rgbs, dict(shDeg=2, tileCull=cull, maxBatch=2),
+                                 radius=1.0)
+        t.iter = 2000
+        for k in range(3):
+            t.stepBatch([0, 1])
+        st = t.readLoss()
+        g = t.readGaussians()
+        m = t.readMoments()
+        res[cull] = (st, g, m, t._state().lastEntries)
+    (st0, g0, m0, e0), (st1, g1, m1, e1) = res[0], res[1]
+    assert e1 < e0, (e1, e0)
+    assert st0 == st1, (st0, st1)
+    assert_bits(g0["data"], g1["data"], "parameters")
+    assert_bits(g0["sh"], g1["sh"], "SH coefficients")
+    for a, b in zip(m0, m1):
+        assert_bits(a, b, "moments")
