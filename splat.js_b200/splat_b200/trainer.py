@@ -53,9 +53,7 @@ def _cam_struct(c, imgIdx=0):
 
 
 # option names of the reference (trainer.js:18-49) -> gs_options fields
-_OPT_FIELDS = ["eCut", "aMin", "radClamp", "anisoReg", "shDeg", "tileGrad", "entriesCap", "maxSplats", "capMult",
-               "maxIters", "minScale", "opacityReg", "shLr", "growRate", "growUntil", "tile", "batchDepth",
-               "maxBatch", "backwardVariant", "persistent", "useGraphs", "device"]
+_OPT_FIELDS = [name for name, _ in N.GsOptions._fields_]
 
 
 class _Queue:
