@@ -45,7 +45,8 @@ def test_static_sort_matches_trainer_binning_twice():
     import torch
     params, sh, cams, rgbs = config0()
     n = len(params) // 16
-    t, targets, metas = make(params, sh, cams, rgbs, dict(shDeg=2), radius=1.0)
+    # full rectangle lists (no tile cull), which host_entries reproduces
+    t, targets, metas = make(params, sh, cams, rgbs, dict(shDeg=2, tileCull=0), radius=1.0)
     gpu_raster(t, [0], 1)
     L = N.lib()
     rect = np.zeros(n * 2, np.uint32)
