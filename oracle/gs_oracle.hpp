@@ -457,33 +457,46 @@ inline Splat2D<T> splat2D(const T* pr) {
 // tile) entry only when some pixel centre of the tile can pass the
 // rasteriser's test e <= eCut and w exp(-e) >= aMin.  The exact minimum of
 // e = hA dx^2 + B dx dy + hC dy^2 over the tile's pixel-centre rectangle is
-// taken in double and compared with min(eCut, eA) (eA = log_f(w / aMin)) plus
-// margins for the FP32 evaluation; the library runs the same sequence, so
-// both keep the same entries.  Culled entries contribute to no pixel.
-inline bool tileLive(float mx, float my, float hA, float B, float hC, float eA, float eCut, int tx, int ty,
-                     int tile, int W, int H) {
-  if (!(hA > 0.0f) || !(hC > 0.0f)) return true;
+// taken in double (edge minima at dy = kx dx, dx = ky dy, clamped) and
+// compared with min(eCut, eA) (eA = log_f(w / aMin)) plus margins for the
+// FP32 evaluation; the library runs the same sequence, so both keep the same
+// entries.  Culled entries contribute to no pixel.  A single-tile rectangle
+// keeps its tile untested.
+struct CullSplat {
+  float mx, my, hA, B, hC, eA;
+  double kx, ky;
+};
+
+inline CullSplat cullPrep(float mx, float my, float hA, float B, float hC, float w, float aMin) {
+  CullSplat s;
+  s.mx = mx; s.my = my; s.hA = hA; s.B = B; s.hC = hC;
+  s.eA = log_f(w / aMin);
+  s.kx = -(double)B / (2.0 * (double)hC);
+  s.ky = -(double)B / (2.0 * (double)hA);
+  return s;
+}
+
+inline bool tileLive(const CullSplat& s, float eCut, int tx, int ty, int tile, int W, int H) {
+  if (!(s.hA > 0.0f) || !(s.hC > 0.0f)) return true;
   const int xe = std::min(tx * tile + tile, W), ye = std::min(ty * tile + tile, H);
-  const double X0 = ((double)(tx * tile) + 0.5) - (double)mx;
-  const double X1 = ((double)(xe - 1) + 0.5) - (double)mx;
-  const double Y0 = ((double)(ty * tile) + 0.5) - (double)my;
-  const double Y1 = ((double)(ye - 1) + 0.5) - (double)my;
-  const double a = hA, b = B, c = hC;
+  const double X0 = ((double)(tx * tile) + 0.5) - (double)s.mx;
+  const double X1 = ((double)(xe - 1) + 0.5) - (double)s.mx;
+  const double Y0 = ((double)(ty * tile) + 0.5) - (double)s.my;
+  const double Y1 = ((double)(ye - 1) + 0.5) - (double)s.my;
+  const double a = s.hA, b = s.B, c = s.hC;
   double emin = 0.0;
   if (!(X0 <= 0.0 && X1 >= 0.0 && Y0 <= 0.0 && Y1 >= 0.0)) {
-    emin = 1.0e300;
-    for (double dx : {X0, X1}) {
-      const double dy = std::fmin(std::fmax(-(b * dx) / (2.0 * c), Y0), Y1);
-      emin = std::fmin(emin, (a * dx) * dx + (b * dx) * dy + (c * dy) * dy);
-    }
-    for (double dy : {Y0, Y1}) {
-      const double dx = std::fmin(std::fmax(-(b * dy) / (2.0 * a), X0), X1);
-      emin = std::fmin(emin, (a * dx) * dx + (b * dx) * dy + (c * dy) * dy);
-    }
+    const double dy0 = std::fmin(std::fmax(s.kx * X0, Y0), Y1), dy1 = std::fmin(std::fmax(s.kx * X1, Y0), Y1);
+    const double dx0 = std::fmin(std::fmax(s.ky * Y0, X0), X1), dx1 = std::fmin(std::fmax(s.ky * Y1, X0), X1);
+    const double e0 = (a * X0) * X0 + (b * X0) * dy0 + (c * dy0) * dy0;
+    const double e1 = (a * X1) * X1 + (b * X1) * dy1 + (c * dy1) * dy1;
+    const double e2 = (a * dx0) * dx0 + (b * dx0) * Y0 + (c * Y0) * Y0;
+    const double e3 = (a * dx1) * dx1 + (b * dx1) * Y1 + (c * Y1) * Y1;
+    emin = std::fmin(std::fmin(e0, e1), std::fmin(e2, e3));
   }
   const double ax = std::fmax(-X0, X1), ay = std::fmax(-Y0, Y1);
   const double smax = (a * ax) * ax + (std::fabs(b) * ax) * ay + (c * ay) * ay;
-  const double thr = std::fmin((double)eCut, (double)eA + 1.0e-5) + 2.0e-6 * smax + 1.0e-6;
+  const double thr = std::fmin((double)eCut, (double)s.eA + 1.0e-5) + 2.0e-6 * smax + 1.0e-6;
   return emin <= thr;
 }
 
@@ -499,17 +512,17 @@ inline Bins binTiles(const Opts& o, const Cam& c, const T* proj, uint32_t n) {
     if (!(pr[11] > T(0))) continue;
     TileRect r = tileRect<T>(c, o.tile, pr[0], pr[1], pr[15]);
     const float depth = (float)pr[2];
-    float cmx = 0, cmy = 0, chA = 0, cB = 0, chC = 0, ceA = 0;
-    if (o.tileCull) {
+    const bool test = o.tileCull && !(r.x0 == r.x1 && r.y0 == r.y1);
+    CullSplat cs{};
+    if (test) {
       const Splat2D<T> s2 = splat2D<T>(pr);
-      cmx = (float)s2.mx; cmy = (float)s2.my;
-      chA = (float)(T(0.5) * s2.cA); cB = (float)s2.cB; chC = (float)(T(0.5) * s2.cC);
-      ceA = log_f((float)s2.w / o.aMin);
+      cs = cullPrep((float)s2.mx, (float)s2.my, (float)(T(0.5) * s2.cA), (float)s2.cB, (float)(T(0.5) * s2.cC),
+                    (float)s2.w, o.aMin);
     }
     for (int y = r.y0; y <= r.y1; ++y)
       for (int x = r.x0; x <= r.x1; ++x) {
         b.cnt[y * tx + x]++;  // the budget counts every rectangle tile
-        if (o.tileCull && !tileLive(cmx, cmy, chA, cB, chC, ceA, o.eCut, x, y, o.tile, c.W, c.H)) continue;
+        if (test && !tileLive(cs, o.eCut, x, y, o.tile, c.W, c.H)) continue;
         lists[y * tx + x].push_back({fbits(depth), i});
       }
   }

@@ -93,43 +93,51 @@ __device__ __forceinline__ float glog(float x) {
 // test (e <= eCut and alpha = w exp(-e) >= aMin) for the splat with mean
 // (mx, my) and conic halves (hA, B, hC)?  The exact minimum of
 // e = hA dx^2 + B dx dy + hC dy^2 over the rectangle of the tile's pixel
-// centres (clipped to the image) is computed in double and compared with
-// min(eCut, ln(w / aMin)) plus margins that cover the rasteriser's FP32
-// evaluation (a few ulp of the largest term, bounded by smax) and the
-// canonical log.  Every pixel that passes the FP32 test lies in a tile that
-// passes this one, so dropping the other entries changes no pixel.  The same
-// double-precision sequence runs in the oracle; results are identical.
-//   eA = glog(w / aMin), computed once per splat.
-__device__ __forceinline__ bool tileLive(float mx, float my, float hA, float B, float hC, float eA, float eCut,
-                                         int tx, int ty, int tile, int W, int H) {
-  if (!(hA > 0.0f) || !(hC > 0.0f)) return true;
+// centres (clipped to the image) is computed in double -- on an edge dx = X
+// the minimum lies at dy = kx X clamped to the edge, kx = -B / (2 hC), and
+// likewise with ky = -B / (2 hA) -- and compared with min(eCut, eA) plus
+// margins that cover the rasteriser's FP32 evaluation (a few ulp of the
+// largest term, bounded by smax) and the canonical log (eA = glog(w / aMin)).
+// Every pixel that passes the FP32 test lies in a tile that passes this one,
+// so dropping the other entries changes no pixel.  The oracle runs the same
+// double-precision sequence, so both keep the same entries.  A splat whose
+// rectangle is a single tile keeps it without the test.
+struct CullSplat {
+  float mx, my, hA, B, hC, eA;
+  double kx, ky;
+};
+
+__device__ __forceinline__ CullSplat cullPrep(float mx, float my, float hA, float B, float hC, float w, float aMin) {
+  CullSplat s;
+  s.mx = mx; s.my = my; s.hA = hA; s.B = B; s.hC = hC;
+  s.eA = glog(w / aMin);
+  s.kx = -(double)B / (2.0 * (double)hC);
+  s.ky = -(double)B / (2.0 * (double)hA);
+  return s;
+}
+
+__device__ __forceinline__ bool tileLive(const CullSplat& s, float eCut, int tx, int ty, int tile, int W, int H) {
+  if (!(s.hA > 0.0f) || !(s.hC > 0.0f)) return true;
   const int xe = tx * tile + tile < W ? tx * tile + tile : W;
   const int ye = ty * tile + tile < H ? ty * tile + tile : H;
-  const double X0 = ((double)(tx * tile) + 0.5) - (double)mx;
-  const double X1 = ((double)(xe - 1) + 0.5) - (double)mx;
-  const double Y0 = ((double)(ty * tile) + 0.5) - (double)my;
-  const double Y1 = ((double)(ye - 1) + 0.5) - (double)my;
-  const double a = (double)hA, b = (double)B, c = (double)hC;
+  const double X0 = ((double)(tx * tile) + 0.5) - (double)s.mx;
+  const double X1 = ((double)(xe - 1) + 0.5) - (double)s.mx;
+  const double Y0 = ((double)(ty * tile) + 0.5) - (double)s.my;
+  const double Y1 = ((double)(ye - 1) + 0.5) - (double)s.my;
+  const double a = (double)s.hA, b = (double)s.B, c = (double)s.hC;
   double emin = 0.0;
   if (!(X0 <= 0.0 && X1 >= 0.0 && Y0 <= 0.0 && Y1 >= 0.0)) {
-    emin = 1.0e300;
-    const double xs[2] = {X0, X1}, ys[2] = {Y0, Y1};
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const double dx = xs[k];
-      const double dy = fmin(fmax(-(b * dx) / (2.0 * c), Y0), Y1);
-      emin = fmin(emin, (a * dx) * dx + (b * dx) * dy + (c * dy) * dy);
-    }
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const double dy = ys[k];
-      const double dx = fmin(fmax(-(b * dy) / (2.0 * a), X0), X1);
-      emin = fmin(emin, (a * dx) * dx + (b * dx) * dy + (c * dy) * dy);
-    }
+    const double dy0 = fmin(fmax(s.kx * X0, Y0), Y1), dy1 = fmin(fmax(s.kx * X1, Y0), Y1);
+    const double dx0 = fmin(fmax(s.ky * Y0, X0), X1), dx1 = fmin(fmax(s.ky * Y1, X0), X1);
+    const double e0 = (a * X0) * X0 + (b * X0) * dy0 + (c * dy0) * dy0;
+    const double e1 = (a * X1) * X1 + (b * X1) * dy1 + (c * dy1) * dy1;
+    const double e2 = (a * dx0) * dx0 + (b * dx0) * Y0 + (c * Y0) * Y0;
+    const double e3 = (a * dx1) * dx1 + (b * dx1) * Y1 + (c * Y1) * Y1;
+    emin = fmin(fmin(e0, e1), fmin(e2, e3));
   }
   const double ax = fmax(-X0, X1), ay = fmax(-Y0, Y1);
   const double smax = (a * ax) * ax + (fabs(b) * ax) * ay + (c * ay) * ay;
-  const double thr = fmin((double)eCut, (double)eA + 1.0e-5) + 2.0e-6 * smax + 1.0e-6;
+  const double thr = fmin((double)eCut, (double)s.eA + 1.0e-5) + 2.0e-6 * smax + 1.0e-6;
   return emin <= thr;
 }
 

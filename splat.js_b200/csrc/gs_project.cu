@@ -244,7 +244,10 @@ __global__ void k_tile_ranges_finish(TileRangeArgs a, uint32_t totalTiles) {
 // KEYS = false counts each item's entries, KEYS = true writes them at the
 // counts' exclusive scan -- key = global tile id, value = splat id, tiles of
 // an item in row order.  An entry is a tile of the item's rectangle that the
-// entry budget kept and, with culling on, that tileLive() accepts.
+// entry budget kept and, with culling on, that tileLive() accepts (a
+// single-tile rectangle is kept untested).  The count pass records the test's
+// results for an item's first 64 candidates in liveMask, which the key pass
+// reads instead of testing again.
 //
 // A warp walks the candidate (item, tile) pairs of its 32 items 32 at a time:
 // each lane finds the item owning its candidate by a binary search over the
@@ -254,7 +257,8 @@ __global__ void k_tile_ranges_finish(TileRangeArgs a, uint32_t totalTiles) {
 // walked by their own lane (rare).
 template <bool KEYS>
 __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
-  __shared__ uint32_t s_run[256];  // entries of each item so far
+  __shared__ uint32_t s_run[256];                 // entries of each item so far
+  __shared__ unsigned long long s_mask[KEYS ? 1 : 256];  // count pass: test results
   const uint64_t items = (uint64_t)a.n * a.V;
   const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
@@ -262,22 +266,25 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
   const uint32_t FULL = 0xFFFFFFFFu;
   const bool valid = p < items;
   uint32_t v = 0, i = 0, x0 = 0, y0 = 0, rw = 1, rc = 0, out = 0;
-  float mx = 0.0f, my = 0.0f, hA = 0.0f, B = 0.0f, hC = 0.0f, eA = 0.0f;
+  bool test = false;
+  unsigned long long mask = 0;
+  CullSplat cs{};
   s_run[threadIdx.x] = 0;
+  if (!KEYS) s_mask[threadIdx.x] = 0;
   if (valid) {
     const uint32_t slot = a.sortedSlots[p];
     const uint2 r = a.rect[slot];
-    if (KEYS) out = a.offsets[p];
+    if (KEYS) { out = a.offsets[p]; if (a.cull) mask = a.liveMask[p]; }
     if (r.x != 0xFFFFFFFFu) {
       v = slot / a.n;
       i = slot - v * a.n;
       x0 = r.x & 0xFFFFu; y0 = r.x >> 16;
       const uint32_t x1 = r.y & 0xFFFFu, y1 = r.y >> 16;
       rw = x1 - x0 + 1;
-      if (a.cull) {
+      test = a.cull && !(x0 == x1 && y0 == y1);
+      if (test) {
         const float4 q0 = a.recs[slot].r0, q1 = a.recs[slot].r1;
-        mx = q0.x; my = q0.y; hA = q0.z; B = q0.w; hC = q1.x;
-        eA = glog(q1.y / a.aMin);
+        cs = cullPrep(q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, a.aMin);
       }
       if (a.viewDrops[v] == 0) {
         rc = rw * (y1 - y0 + 1);
@@ -289,7 +296,7 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
           for (uint32_t x = x0; x <= x1; ++x) {
             const uint32_t t = y * c.tilesX + x;
             if (dr[t]) continue;
-            if (a.cull && !tileLive(mx, my, hA, B, hC, eA, a.eCut, (int)x, (int)y, a.tile, c.W, c.H)) continue;
+            if (test && !tileLive(cs, a.eCut, (int)x, (int)y, a.tile, c.W, c.H)) continue;
             if (KEYS) {
               if (o < a.capacity) { a.keys[o] = c.tileBase + t; a.vals[o] = i; }
               else atomicOr(a.status, ST_ENTRY_OVERFLOW);
@@ -330,21 +337,28 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
     const uint32_t ov = __shfl_sync(FULL, v, lo);
     const uint32_t oi = __shfl_sync(FULL, i, lo);
     const uint32_t oout = __shfl_sync(FULL, out, lo);
-    const float omx = __shfl_sync(FULL, mx, lo);
-    const float omy = __shfl_sync(FULL, my, lo);
-    const float ohA = __shfl_sync(FULL, hA, lo);
-    const float oB = __shfl_sync(FULL, B, lo);
-    const float ohC = __shfl_sync(FULL, hC, lo);
-    const float oeA = __shfl_sync(FULL, eA, lo);
+    const bool otest = __shfl_sync(FULL, (uint32_t)test, lo) != 0u;
+    const unsigned long long omask = KEYS ? __shfl_sync(FULL, mask, lo) : 0ull;
+    CullSplat ocs;
+    ocs.mx = __shfl_sync(FULL, cs.mx, lo);
+    ocs.my = __shfl_sync(FULL, cs.my, lo);
+    ocs.hA = __shfl_sync(FULL, cs.hA, lo);
+    ocs.B = __shfl_sync(FULL, cs.B, lo);
+    ocs.hC = __shfl_sync(FULL, cs.hC, lo);
+    ocs.eA = __shfl_sync(FULL, cs.eA, lo);
+    ocs.kx = __shfl_sync(FULL, cs.kx, lo);
+    ocs.ky = __shfl_sync(FULL, cs.ky, lo);
     bool live = false;
-    uint32_t gt = 0;
+    uint32_t gt = 0, k = 0;
     if (inRange) {
-      const uint32_t k = e - ocb;
+      k = e - ocb;
       const uint32_t ry = k / orw, rx = k - ry * orw;
       const uint32_t tx = ox + rx, ty = oy + ry;
       const DevCam& c = a.cams[ov];
       gt = c.tileBase + ty * (uint32_t)c.tilesX + tx;
-      live = !a.cull || tileLive(omx, omy, ohA, oB, ohC, oeA, a.eCut, (int)tx, (int)ty, a.tile, c.W, c.H);
+      if (!otest) live = true;
+      else if (KEYS && k < 64) live = ((omask >> k) & 1ull) != 0ull;
+      else live = tileLive(ocs, a.eCut, (int)tx, (int)ty, a.tile, c.W, c.H);
     }
     const uint32_t lb = __ballot_sync(FULL, live);
     const uint32_t peers = __match_any_sync(FULL, inRange ? (uint32_t)lo : 32u);
@@ -355,10 +369,18 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
       else atomicOr(a.status, ST_ENTRY_OVERFLOW);
     }
     __syncwarp();
-    if (inRange && lane == __ffs(peers) - 1) s_run[wbase + lo] = prior + __popc(lb & peers);
+    const int lead = __ffs(peers) - 1;
+    if (inRange && lane == lead) {
+      s_run[wbase + lo] = prior + __popc(lb & peers);
+      // the group's candidates are consecutive: bit j of (lb & peers) >> lead is candidate k + j
+      if (!KEYS && k < 64) s_mask[wbase + lo] |= (unsigned long long)((lb & peers) >> lead) << k;
+    }
     __syncwarp();
   }
-  if (!KEYS && valid) a.counts[p] = s_run[threadIdx.x];
+  if (!KEYS && valid) {
+    a.counts[p] = s_run[threadIdx.x];
+    if (a.cull) a.liveMask[p] = s_mask[threadIdx.x];
+  }
 }
 
 // Per-tile ranges from the sorted entry keys (culled lists): tile gt spans

@@ -77,6 +77,7 @@ struct gs_trainer {
   RenderRec* recs = nullptr;
   uint2* rect = nullptr;
   uint32_t *counts = nullptr, *offsets = nullptr;
+  unsigned long long* liveMask = nullptr;
   int32_t* gradP = nullptr;
   int32_t* diffGrid = nullptr;
   uint32_t* tileCnt = nullptr;
@@ -379,6 +380,7 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   GS_AL(h->rect, (size_t)B * cap);
   GS_AL(h->counts, (size_t)B * cap);
   GS_AL(h->offsets, (size_t)B * cap);
+  GS_AL(h->liveMask, (size_t)B * cap);
   GS_AL(h->gradP, (size_t)B * cap * GP_STRIDE);
   // (tx+1)(ty+1) = tiles + tx + ty + 1 <= 3 * maxTiles + 1 for any view of at most maxTiles tiles
   GS_AL(h->diffGrid, (size_t)B * (3 * (size_t)h->maxTiles + 1));
@@ -628,6 +630,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   ea.tile = sh.tile;
   ea.cull = cull ? 1 : 0;
   ea.counts = h->counts;
+  ea.liveMask = h->liveMask;
   ea.offsets = h->offsets;
   ea.keys = h->keys[0];
   ea.vals = h->vals[0];
