@@ -135,17 +135,40 @@ __global__ void __launch_bounds__(1024) k_tile_counts(TileRangeArgs a) {
   const DevCam c = a.cams[v];
   const int tx = c.tilesX, ty = c.tilesY, gw = tx + 1;
   int32_t* gd = a.diffGrid + a.gridBase[v];
-  // rows: prefix along x
-  for (int y = threadIdx.x; y < ty; y += blockDim.x) {
-    int32_t acc = 0;
-    for (int x = 0; x < tx; ++x) { acc += gd[y * gw + x]; gd[y * gw + x] = acc; }
+  // rows: prefix along x, one warp per row, 32 columns per step
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int y = wid; y < ty; y += nw) {
+    int32_t carry = 0;
+    for (int x0 = 0; x0 < tx; x0 += 32) {
+      const int x = x0 + lane;
+      int32_t v = x < tx ? gd[y * gw + x] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int32_t u = __shfl_up_sync(0xFFFFFFFFu, v, o);
+        if (lane >= o) v += u;
+      }
+      v += carry;
+      if (x < tx) gd[y * gw + x] = v;
+      carry = __shfl_sync(0xFFFFFFFFu, v, 31);
+    }
   }
   __syncthreads();
-  // columns: prefix along y -> per-tile count
+  // columns: prefix along y -> per-tile count, one warp per column
   uint32_t* cnt = a.tileCnt + c.tileBase;
-  for (int x = threadIdx.x; x < tx; x += blockDim.x) {
-    int32_t acc = 0;
-    for (int y = 0; y < ty; ++y) { acc += gd[y * gw + x]; cnt[y * tx + x] = (uint32_t)acc; }
+  for (int x = wid; x < tx; x += nw) {
+    int32_t carry = 0;
+    for (int y0 = 0; y0 < ty; y0 += 32) {
+      const int y = y0 + lane;
+      int32_t v = y < ty ? gd[y * gw + x] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int32_t u = __shfl_up_sync(0xFFFFFFFFu, v, o);
+        if (lane >= o) v += u;
+      }
+      v += carry;
+      if (y < ty) cnt[y * tx + x] = (uint32_t)v;
+      carry = __shfl_sync(0xFFFFFFFFu, v, 31);
+    }
   }
   __syncthreads();
   // budget: padded prefix; fast path when the whole view fits
@@ -191,7 +214,6 @@ __global__ void __launch_bounds__(1024) k_tile_counts(TileRangeArgs a) {
   const int t0 = threadIdx.x * per;
   uint32_t mine = 0;
   for (int t = t0; t < min(nt, t0 + per); ++t) mine += dr[t] ? 0u : cnt[t];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   uint32_t inc = mine;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
