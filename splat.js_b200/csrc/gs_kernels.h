@@ -22,6 +22,7 @@ struct ProjectArgs {
   uint2* rect;             // V * n
   int32_t* diffGrid;       // per view (tilesX+1)*(tilesY+1), cleared before
   const uint32_t* gridBase;  // V offsets into diffGrid
+  float4* cullRecs;        // V * n warp-block cull parameters (p, q, kA, 0)
 };
 
 struct TileRangeArgs {
@@ -103,6 +104,7 @@ struct RasterArgs {
   int V;
   uint32_t n;
   const RenderRec* recs;   // V * n
+  const float4* cullRecs;  // V * n warp-block cull parameters
   const uint32_t* ids;     // sorted entry values (splat ids)
   const uint2* ranges;     // per global tile
   uint32_t totalTiles;

@@ -114,6 +114,31 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
     const uint32_t y0 = u32sat(clampf(floorf((my - rad) / TF), 0.0f, (float)(ty - 1)));
     const uint32_t y1 = u32sat(clampf(floorf((my + rad) / TF), 0.0f, (float)(ty - 1)));
     a.rect[slot] = make_uint2(x0 | (y0 << 16), x1 | (y1 << 16));
+    // warp-block cull parameters, read when the rasteriser stages the entry.
+    // Completing the square in dx, a pixel (dx, dy) with exact exponent
+    // e <= t satisfies |dx - kA dy| <= sqrt(p - q dy^2), kA = -B / (2 hA),
+    // p = t / hA, q = (4 hA hC - B^2) / (4 hA^2).  t is the largest exponent
+    // the rasteriser can accept, min(eCut, ln(w / aMin)), plus margins for its
+    // FP32 evaluation (a few ulp of the largest term over the rectangle).  p
+    // is rounded up and q down, so the bound stays conservative; +inf = keep
+    // every warp (degenerate conic).
+    {
+      float4 cq = make_float4(__int_as_float(0x7F800000), 0.0f, 0.0f, 0.0f);
+      const double A = (double)r.r0.z, Bq = (double)r.r0.w, Cq = (double)r.r1.x;
+      const double det = 4.0 * A * Cq - Bq * Bq;
+      if (A > 0.0 && Cq > 0.0 && det > 0.0) {
+        const double dmx = (double)mx, dmy = (double)my, T = (double)a.tile;
+        const double ax = fmax(dmx - (double)x0 * T, (double)(x1 + 1) * T - dmx);
+        const double ay = fmax(dmy - (double)y0 * T, (double)(y1 + 1) * T - dmy);
+        const double smax = (A * ax) * ax + (fabs(Bq) * ax) * ay + (Cq * ay) * ay;
+        const double eA = (double)glog(r.r1.y / a.aMin);
+        const double tmax = fmin((double)a.eCut, eA + 1.0e-5) + 2.0e-6 * smax + 1.0e-6;
+        cq.x = __double2float_ru(tmax / A);
+        cq.y = __double2float_rd(det / (4.0 * A * A));
+        cq.z = __double2float_rn(-Bq / (2.0 * A));
+      }
+      a.cullRecs[slot] = cq;
+    }
     // rectangle add on the (tx+1) x (ty+1) difference grid
     int32_t* gd = a.diffGrid + a.gridBase[v];
     const int gw = tx + 1;

@@ -58,6 +58,43 @@ __device__ __forceinline__ bool warpTouches(const float4& r0, float cullR, float
   return ox * ox + oy * oy <= cullR * cullR;
 }
 
+// Which of the tile's 8x4 warp blocks can the splat reach?  Bit w = warp w
+// (block row w / (TILE/8), column w % (TILE/8)).  For each 4-row band, the
+// splat's pixels lie within |dx - kA dy| <= sqrt(p - q dmin^2) (cull
+// parameters (p, q, kA) from the projection; dmin = the band's smallest |dy|),
+// an x interval checked against each block of the band.  Slack covers this
+// FP32 evaluation, so a cleared bit means no pixel of the block can pass the
+// rasteriser's cutoffs: skipping the entry there changes nothing.
+template <int TILE>
+__device__ __forceinline__ uint32_t warp_block_mask(const float4 cq, float mx, float my, int tx, int ty) {
+  constexpr int NB = TILE / 4, WPR = TILE / 8;
+  constexpr uint32_t ALL = NB * WPR >= 32 ? 0xFFFFFFFFu : (1u << (NB * WPR)) - 1u;
+  if (!(cq.x < 3.0e38f)) return ALL;
+  const float p = cq.x, q = cq.y, kA = cq.z;
+  const float slackA = 4.0e-3f * (1.0f + fabsf(kA));
+  uint32_t m = 0;
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    const float Y0 = ((float)(ty * TILE + 4 * b) + 0.5f) - my;
+    const float Y1 = Y0 + 3.0f;
+    float d = Y0 > 0.0f ? Y0 : (Y1 < 0.0f ? -Y1 : 0.0f);
+    d = fmaxf(d - (1.0e-3f + 1.0e-6f * d), 0.0f);
+    const float rad2 = __fmaf_rn(-q, d * d, p) + 1.0e-5f * p;
+    if (!(rad2 >= 0.0f)) continue;
+    const float r = sqrtf(rad2) * 1.00001f;
+    const float c0 = kA * Y0, c1 = kA * Y1;
+    const float cl = fminf(c0, c1), ch = fmaxf(c0, c1);
+    const float sl = slackA + 1.0e-5f * (fabsf(cl) + fabsf(ch) + r);
+    const float xl = (cl - r) - sl, xr = (ch + r) + sl;
+#pragma unroll
+    for (int wb = 0; wb < WPR; ++wb) {
+      const float bx0 = ((float)(tx * TILE + 8 * wb) + 0.5f) - mx;
+      if (bx0 + 7.0f >= xl && bx0 <= xr) m |= 1u << (b * WPR + wb);
+    }
+  }
+  return m;
+}
+
 // TILE x TILE pixels per CTA, one per thread; warps cover 8x4 blocks.
 template <int TILE, int BATCH, bool FWD, bool BWD, bool STORED>
 __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
@@ -71,6 +108,7 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
   __shared__ uint32_t s_id[BATCH];
   __shared__ int32_t s_acc[BWD ? BATCH * 10 : 1];
   __shared__ uint32_t s_mask[MASKS ? NW * MASKW : 1];
+  __shared__ uint32_t s_live[FWD ? NW : 1][BATCH / 32];  // per warp: staged entries its block can reach
   __shared__ uint32_t s_item;
   __shared__ uint32_t s_redu[NW][5];
   __shared__ uint32_t s_endmax[NW];
@@ -107,6 +145,7 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
     const uint32_t s = rg.x, e = rg.y;
     const size_t pix = (size_t)c.pixBase + (size_t)y * c.W + x;
     const RenderRec* recs = a.recs + (size_t)v * a.n;
+    const float4* cullRecs = a.cullRecs + (size_t)v * a.n;
 
     float T = 1.0f;
     float C0 = 0.0f, C1 = 0.0f, C2 = 0.0f;
@@ -120,18 +159,35 @@ __global__ void __launch_bounds__(TILE * TILE) k_raster(RasterArgs a) {
       for (uint32_t base = s; base < e; base += BATCH) {
         if (__syncthreads_count(!done) == 0) break;
         const uint32_t nb = min((uint32_t)BATCH, e - base);
-        for (uint32_t k = tid; k < nb; k += RTHREADS) {
-          const uint32_t id = a.ids[base + k];
-          s_id[k] = id;
-          s_rec[k] = recs[id];
+        // stage the batch; each staging thread also finds which warp blocks
+        // its entry can reach, and a ballot per warp block transposes that
+        // into one word per 32 entries
+        for (uint32_t kb = 0; kb < (uint32_t)BATCH; kb += RTHREADS) {
+          const uint32_t k = kb + tid;
+          uint32_t m = 0;
+          if (k < nb) {
+            const uint32_t id = a.ids[base + k];
+            s_id[k] = id;
+            const RenderRec rec = recs[id];
+            s_rec[k] = rec;
+            m = warp_block_mask<TILE>(cullRecs[id], rec.r0.x, rec.r0.y, tx, ty);
+          }
+          const uint32_t word = (kb >> 5) + (uint32_t)wid;
+#pragma unroll
+          for (int w = 0; w < NW; ++w) {
+            const uint32_t bw = __ballot_sync(FULL, (m >> w) & 1u);
+            if (lane == 0 && word < (uint32_t)(BATCH / 32)) s_live[w][word] = bw;
+          }
         }
         __syncthreads();
         if (!__all_sync(FULL, done)) {
           const uint32_t rbase = base - s;
           for (uint32_t jw = 0; jw < nb; jw += 32) {  // one ballot word per 32 entries
-            const uint32_t jn = min(32u, nb - jw);
+            uint32_t live = s_live[wid][jw >> 5];  // entries this warp's block can reach
             uint32_t bits = 0;
-            for (uint32_t jj = 0; jj < jn; ++jj) {
+            while (live) {
+              const uint32_t jj = (uint32_t)__ffs(live) - 1u;
+              live &= live - 1u;
               const RenderRec& rr = s_rec[jw + jj];
               const float4 r0 = rr.r0;
               const float4 r1 = rr.r1;

@@ -78,6 +78,7 @@ struct gs_trainer {
   uint2* rect = nullptr;
   uint32_t *counts = nullptr, *offsets = nullptr;
   unsigned long long* liveMask = nullptr;
+  float4* cullRecs = nullptr;
   int32_t* gradP = nullptr;
   int32_t* diffGrid = nullptr;
   uint32_t* tileCnt = nullptr;
@@ -381,6 +382,7 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   GS_AL(h->counts, (size_t)B * cap);
   GS_AL(h->offsets, (size_t)B * cap);
   GS_AL(h->liveMask, (size_t)B * cap);
+  GS_AL(h->cullRecs, (size_t)B * cap);
   GS_AL(h->gradP, (size_t)B * cap * GP_STRIDE);
   // (tx+1)(ty+1) = tiles + tx + ty + 1 <= 3 * maxTiles + 1 for any view of at most maxTiles tiles
   GS_AL(h->diffGrid, (size_t)B * (3 * (size_t)h->maxTiles + 1));
@@ -576,6 +578,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   pa.rect = h->rect;
   pa.diffGrid = h->diffGrid;
   pa.gridBase = h->dParams->gridBase;
+  pa.cullRecs = h->cullRecs;
   launch_project(pa, h->o.shDeg, s);
 
   TileRangeArgs ta{};
@@ -677,6 +680,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   rr.V = V;
   rr.n = sh.n;
   rr.recs = h->recs;
+  rr.cullRecs = h->cullRecs;
   rr.ids = sortedIds;
   rr.ranges = h->ranges;
   rr.totalTiles = totalTiles;

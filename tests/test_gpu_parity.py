@@ -419,3 +419,17 @@ def test_tile_cull_changes_no_training_result():
     assert_bits(g0["sh"], g1["sh"], "SH coefficients")
     for a, b in zip(m0, m1):
         assert_bits(a, b, "moments")
+
+
+@pytest.mark.parametrize("tile", [8, 16, 32])
+def test_needles_and_discs_bitexact(tile):
+    """Strongly anisotropic splats at every orientation: the tile cull and the
+    rasteriser's warp-block skipping must keep every contributing pair."""
+    from test_tile_cull import anisotropic_scene
+    n = 4000
+    params, cam = anisotropic_scene(n, 21 + tile)
+    sh = np.zeros(n * 3 * 8, np.float32)
+    opts = dict(shDeg=2, tile=tile)
+    t, targets, metas = make(params, sh, [cam], [scene.uniform_target(256, 256, seed=21)], opts, radius=1.0)
+    gpu_raster(t, [0], 3)
+    check_view_against_oracle(t, oracle_opts(opts), oracle_cam(metas[0], 0, 1, 2), params, sh, targets, n)
