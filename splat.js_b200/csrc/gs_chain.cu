@@ -2,13 +2,15 @@
 // screen-space gradients to parameter gradients (shaders.js:704-949), fused
 // with Adam (shaders.js:984-1036) and SH-Adam (shaders.js:952-982).
 //
-// One thread per splat.  For a batch of V views, each view's fixed-point
-// screen-space gradients are decoded (and cleared for the next step), chained
-// through that view's camera, and the parameter gradients summed in view
-// order; Adam then updates the splat once.  The reference runs chain, Adam
-// and SH-Adam as three dispatches with gradF / shGrad round-tripping through
-// memory; here they stay in registers unless the caller asks for them
-// (gradient readout for checks).  Operation order follows the WGSL.
+// Two passes.  Pass 1 (one thread per (view, splat)) decodes each visible
+// splat's fixed-point screen-space gradients (clearing them for the next
+// step) and chains them through that view's camera.  Pass 2 (one thread per
+// splat) sums the views' parameter gradients in view order and runs Adam
+// and SH-Adam once, with coalesced parameter and moment traffic.  The
+// reference runs chain, Adam and SH-Adam as three dispatches with gradF /
+// shGrad round-tripping through memory; here the summed gradients stay on
+// chip unless the caller asks for them (gradient readout for checks).
+// Operation order follows the WGSL.
 #include "gs_geom.cuh"
 #include "gs_kernels.h"
 
@@ -25,7 +27,7 @@ struct CamGrad7 {
 template <int DEG>
 __device__ __forceinline__ void chainOne(const DevCam& c, const float* P, const Geom& g, float gp[10],
                                          const float* shp, float anisoReg, float gF[16], float dRGBo[3],
-                                         float Yo[15], int& aKo, CamGrad7& cg) {
+                                         float Yo[15], float vdo[3], int& aKo, CamGrad7& cg) {
   constexpr int K = DEG > 0 ? (DEG + 1) * (DEG + 1) - 1 : 0;
   const float f = c.f, z = g.pc[2], iz = 1.0f / z;
   // conic -> dilated 2D covariance (shaders.js:758-777)
@@ -177,6 +179,7 @@ __device__ __forceinline__ void chainOne(const DevCam& c, const float* P, const 
     const float un[3] = {P[0] - cp[0], P[1] - cp[1], P[2] - cp[2]};
     const float ulen = fmaxf(sqrtf(dot3(un, un)), 1e-9f);
     const float vd[3] = {un[0] / ulen, un[1] / ulen, un[2] / ulen};
+    vdo[0] = vd[0]; vdo[1] = vd[1]; vdo[2] = vd[2];
     shBasis<DEG>(vd, Yo);
     const int aK = shActiveK(c, K);
     aKo = aK;
@@ -227,49 +230,30 @@ __device__ __forceinline__ void adamParam(const AdamHP& h, int slot, float& p, f
   p = pn;
 }
 
-// MULTI: several views are summed (accumulators held per splat); a single
-// view needs none.
-template <int DEG, bool MULTI>
-__global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
+#ifndef GS_CHAIN_MIN_BLOCKS
+#define GS_CHAIN_MIN_BLOCKS 1  // resident 128-thread blocks per SM the register allocation must allow
+#endif
+
+// Pass 1: one thread per (view, splat).  Blocks are ordered splat block major,
+// view minor, so the views of a splat block run together and its parameters
+// and SH coefficients are read from DRAM once.  A visible splat's screen-space
+// gradients are decoded (and cleared for the next step) and chained through
+// the view's camera; the result -- the 14 parameter gradients, the gated
+// colour gradient dRGB and the view direction (from which the SH basis Y is
+// recomputed) -- goes to viewGrad[slot] for pass 2.  Camera gradients are
+// summed per warp in fixed point (order-independent) with one atomic each.
+template <int DEG>
+__global__ void __launch_bounds__(128, GS_CHAIN_MIN_BLOCKS) k_chain_view(ChainArgs a) {
   constexpr int K = DEG > 0 ? (DEG + 1) * (DEG + 1) - 1 : 0;
-  constexpr int SHN = 3 * K > 0 ? 3 * K : 1;
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = i < a.n;
+  const uint32_t sb = blockIdx.x / (uint32_t)a.V;
+  const int v = (int)(blockIdx.x - sb * (uint32_t)a.V);
+  const uint32_t i = sb * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
-
-  float P[16];
-  float gFa[16];
-  float shA[MULTI ? SHN : 1];
-  float dRGB1[3] = {0.0f, 0.0f, 0.0f};  // single view: SH gradient factors
-  float Y1[15];
-  int aK1 = 0;
-#pragma unroll
-  for (int k = 0; k < 16; ++k) { P[k] = 0.0f; gFa[k] = 0.0f; }
-  if (MULTI) {
-#pragma unroll
-    for (int k = 0; k < SHN; ++k) shA[k] = 0.0f;
-  }
-  if (valid) {
-    const float4* P4 = reinterpret_cast<const float4*>(a.params + (size_t)i * STRIDE);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const float4 t = P4[k];
-      P[4 * k] = t.x; P[4 * k + 1] = t.y; P[4 * k + 2] = t.z; P[4 * k + 3] = t.w;
-    }
-  }
-  const float* shp = (K > 0 && valid) ? a.sh + (size_t)i * 3 * K : nullptr;
-
-  for (int v = 0; v < a.V; ++v) {
-    const DevCam& c = a.cams[v];
-    float gF[16];
-#pragma unroll
-    for (int k = 0; k < 16; ++k) gF[k] = 0.0f;
-    float dRGB[3] = {0.0f, 0.0f, 0.0f};
-    float Y[15];
-    int aK = 0;
-    CamGrad7 cg = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f};
-    if (valid) {
-      const size_t slot = (size_t)v * a.n + i;
+  const DevCam& c = a.cams[v];
+  CamGrad7 cg = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f};
+  if (i < a.n) {
+    const size_t slot = (size_t)v * a.n + i;
+    if (a.rect[slot].x != 0xFFFFFFFFu) {
       int4* G4 = reinterpret_cast<int4*>(a.gradP + slot * GP_STRIDE);
       const int4 q0 = G4[0], q1 = G4[1], q2 = G4[2];
       G4[0] = make_int4(0, 0, 0, 0);
@@ -279,122 +263,147 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
       float gp[10];
 #pragma unroll
       for (int k = 0; k < 10; ++k) gp[k] = (float)qi[k] / ((k >= 2 && k <= 4) ? FIXEDC : FIXED);
-      if (a.rect[slot].x != 0xFFFFFFFFu) {
-        const Geom g = computeGeom(c, P);
-        if (g.ok) {
-          // undo the render pass's conic normalisation (shaders.js:735-744)
-          const float cva = g.va + 0.3f, cvc = g.vc + 0.3f;
-          const float cmid = 0.5f * (cva + cvc);
-          const float lmax = cmid + sqrtf(fmaxf(cmid * cmid - (cva * cvc - g.vb * g.vb), 0.0f));
-          const float cden = 1.0f + lmax;
-          gp[2] = gp[2] * cden; gp[3] = gp[3] * cden; gp[4] = gp[4] * cden;
-          chainOne<DEG>(c, P, g, gp, shp, a.anisoReg, gF, dRGB, Y, aK, cg);
-        }
+      float P[16];
+      const float4* P4 = reinterpret_cast<const float4*>(a.params + (size_t)i * STRIDE);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float4 t = __ldg(P4 + k);
+        P[4 * k] = t.x; P[4 * k + 1] = t.y; P[4 * k + 2] = t.z; P[4 * k + 3] = t.w;
+      }
+      float gF[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) gF[k] = 0.0f;
+      float dRGB[3] = {0.0f, 0.0f, 0.0f}, vd[3] = {0.0f, 0.0f, 0.0f}, Y[15];
+      int aK = 0;
+      const Geom g = computeGeom(c, P);
+      if (g.ok) {
+        // undo the render pass's conic normalisation (shaders.js:735-744)
+        const float cva = g.va + 0.3f, cvc = g.vc + 0.3f;
+        const float cmid = 0.5f * (cva + cvc);
+        const float lmax = cmid + sqrtf(fmaxf(cmid * cmid - (cva * cvc - g.vb * g.vb), 0.0f));
+        const float cden = 1.0f + lmax;
+        gp[2] = gp[2] * cden; gp[3] = gp[3] * cden; gp[4] = gp[4] * cden;
+        const float* shp = K > 0 ? a.sh + (size_t)i * 3 * K : nullptr;
+        chainOne<DEG>(c, P, g, gp, shp, a.anisoReg, gF, dRGB, Y, vd, aK, cg);
+      }
+      float4* o = reinterpret_cast<float4*>(a.viewGrad + slot * VIEWGRAD_STRIDE);
+      o[0] = make_float4(gF[0], gF[1], gF[2], gF[3]);
+      o[1] = make_float4(gF[4], gF[5], gF[6], gF[7]);
+      o[2] = make_float4(gF[8], gF[9], gF[10], gF[11]);
+      o[3] = make_float4(gF[12], gF[13], dRGB[0], dRGB[1]);
+      o[4] = make_float4(dRGB[2], vd[0], vd[1], vd[2]);
+    }
+  }
+  // camera gradients: warp sums of the fixed-point values, one atomic each
+  if (c.train) {
+    const float cv[7] = {cg.w[0], cg.w[1], cg.w[2], cg.t[0], cg.t[1], cg.t[2], cg.logf};
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+      const uint32_t r = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)fixq(cv[k], FIXCAM));
+      if (lane == 0 && r) {
+        const uint32_t idx = k < 6 ? c.camIdx * 8u + (uint32_t)k : c.ncams * 8u;
+        atomicAdd(&a.gradCam[idx], (int32_t)r);
       }
     }
-    // camera gradients: warp sums of the fixed-point values, one atomic each
-    if (c.train) {
-      const float cv[7] = {cg.w[0], cg.w[1], cg.w[2], cg.t[0], cg.t[1], cg.t[2], cg.logf};
-#pragma unroll
-      for (int k = 0; k < 7; ++k) {
-        const uint32_t r = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)fixq(cv[k], FIXCAM));
-        if (lane == 0 && r) {
-          const uint32_t idx = k < 6 ? c.camIdx * 8u + (uint32_t)k : c.ncams * 8u;
-          atomicAdd(&a.gradCam[idx], (int32_t)r);
-        }
-      }
-    }
-    // parameter gradients summed in view order from 0 (as the oracle sums)
-#pragma unroll
-    for (int k = 0; k < 16; ++k) gFa[k] = gFa[k] + gF[k];
-    if (MULTI) {
-#pragma unroll
-      for (int k = 0; k < K; ++k)
-#pragma unroll
-        for (int ch = 0; ch < 3; ++ch)
-          shA[ch * K + k] = shA[ch * K + k] + (k < aK ? dRGB[ch] * Y[k] : 0.0f);
-    } else {
-      dRGB1[0] = dRGB[0]; dRGB1[1] = dRGB[1]; dRGB1[2] = dRGB[2];
-#pragma unroll
-      for (int k = 0; k < K; ++k) Y1[k] = Y[k];
-      aK1 = aK;
-    }
-  }
-  if (!valid) return;
-  // SH coefficient gradient of (channel, k)
-  auto shGradOf = [&](int ch, int k) -> float {
-    if (MULTI) return shA[ch * K + k];
-    return 0.0f + (k < aK1 ? dRGB1[ch] * Y1[k] : 0.0f);
-  };
-  if (a.gradF) {
-    float4* o = reinterpret_cast<float4*>(a.gradF + (size_t)i * STRIDE);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) o[k] = make_float4(gFa[4 * k], gFa[4 * k + 1], gFa[4 * k + 2], gFa[4 * k + 3]);
-    if (K > 0) {
-      float* so = a.shGrad + (size_t)i * 3 * K;
-#pragma unroll
-      for (int ch = 0; ch < 3; ++ch)
-#pragma unroll
-        for (int k = 0; k < K; ++k) so[ch * K + k] = shGradOf(ch, k);
-    }
-  }
-  if (!a.doAdam) return;
-  float4* M4 = reinterpret_cast<float4*>(a.m + (size_t)i * STRIDE);
-  float4* V4 = reinterpret_cast<float4*>(a.v + (size_t)i * STRIDE);
-  float m[16], vv[16];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const float4 mm = M4[k], vq = V4[k];
-    m[4 * k] = mm.x; m[4 * k + 1] = mm.y; m[4 * k + 2] = mm.z; m[4 * k + 3] = mm.w;
-    vv[4 * k] = vq.x; vv[4 * k + 1] = vq.y; vv[4 * k + 2] = vq.z; vv[4 * k + 3] = vq.w;
-  }
-  const AdamHP hpv = *a.hp;
-#pragma unroll
-  for (int s = 0; s < 16; ++s) adamParam(hpv, s, P[s], gFa[s], m[s], vv[s]);
-  float4* P4o = reinterpret_cast<float4*>(a.params + (size_t)i * STRIDE);
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    P4o[k] = make_float4(P[4 * k], P[4 * k + 1], P[4 * k + 2], P[4 * k + 3]);
-    M4[k] = make_float4(m[4 * k], m[4 * k + 1], m[4 * k + 2], m[4 * k + 3]);
-    V4[k] = make_float4(vv[4 * k], vv[4 * k + 1], vv[4 * k + 2], vv[4 * k + 3]);
-  }
-  if (K > 0) {
-    float* shw = a.sh + (size_t)i * 3 * K;
-    float* shm = a.shM + (size_t)i * 3 * K;
-    float* shv = a.shV + (size_t)i * 3 * K;
-    const AdamHP& h = hpv;
-#pragma unroll
-    for (int ch = 0; ch < 3; ++ch)
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const int j = ch * K + k;
-        float g = shGradOf(ch, k);
-        if (!(fabsf(g) < 1e18f)) g = 0.0f;
-        const float mk = h.b1 * shm[j] + (1.0f - h.b1) * g;
-        const float vk = h.b2 * shv[j] + (1.0f - h.b2) * g * g;
-        shm[j] = mk;
-        shv[j] = vk;
-        const float mh = mk / h.bc1, vh = vk / h.bc2;
-        shw[j] = shw[j] - h.shLr * mh / (sqrtf(vh) + h.eps);
-      }
   }
 }
 
-template <bool MULTI>
-static void launch_chain_t(const ChainArgs& a, int deg, unsigned grid, cudaStream_t s) {
-  switch (deg) {
-    case 0: k_chain_adam<0, MULTI><<<grid, 128, 0, s>>>(a); break;
-    case 1: k_chain_adam<1, MULTI><<<grid, 128, 0, s>>>(a); break;
-    case 2: k_chain_adam<2, MULTI><<<grid, 128, 0, s>>>(a); break;
-    default: k_chain_adam<3, MULTI><<<grid, 128, 0, s>>>(a); break;
+// Pass 2: one thread per splat sums its views' gradients in view order from
+// zero (views where the splat was not visible add +0, which changes no sum,
+// and are skipped), then the block updates its 128 splats with Adam and
+// SH-Adam through shared memory, one float per thread per step, so every
+// global access is coalesced.
+template <int DEG>
+__global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
+  constexpr int K = DEG > 0 ? (DEG + 1) * (DEG + 1) - 1 : 0;
+  constexpr int SHN = 3 * K;
+  constexpr int GROW = 17;                 // padded rows: conflict-free column writes
+  constexpr int SROW = SHN > 0 ? SHN + 1 : 1;
+  constexpr uint32_t SHD = SHN > 0 ? SHN : 1;  // divisor (the SH loops are empty when SHN = 0)
+  __shared__ float s_g[128 * GROW];
+  __shared__ float s_sh[SHN > 0 ? 128 * SROW : 1];
+  const uint32_t i0 = blockIdx.x * blockDim.x;
+  const uint32_t i = i0 + threadIdx.x;
+  const int t = threadIdx.x;
+  {
+    float gFa[14];
+    float shA[SHN > 0 ? SHN : 1];
+#pragma unroll
+    for (int k = 0; k < 14; ++k) gFa[k] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < SHN; ++k) shA[k] = 0.0f;
+    if (i < a.n) {
+      for (int v = 0; v < a.V; ++v) {
+        const size_t slot = (size_t)v * a.n + i;
+        if (a.rect[slot].x == 0xFFFFFFFFu) continue;
+        const float4* q = reinterpret_cast<const float4*>(a.viewGrad + slot * VIEWGRAD_STRIDE);
+        const float4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
+        const float gF[14] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w,
+                              q2.x, q2.y, q2.z, q2.w, q3.x, q3.y};
+#pragma unroll
+        for (int k = 0; k < 14; ++k) gFa[k] = gFa[k] + gF[k];
+        if (K > 0) {
+          const float4 q4 = q[4];
+          const float dRGB[3] = {q3.z, q3.w, q4.x};
+          const float vd[3] = {q4.y, q4.z, q4.w};
+          float Y[15];
+          shBasis<DEG>(vd, Y);
+          const int aK = shActiveK(a.cams[v], K);
+#pragma unroll
+          for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+              shA[ch * K + k] = shA[ch * K + k] + (k < aK ? dRGB[ch] * Y[k] : 0.0f);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 14; ++k) s_g[t * GROW + k] = gFa[k];
+    s_g[t * GROW + 14] = 0.0f;
+    s_g[t * GROW + 15] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < SHN; ++k) s_sh[t * SROW + k] = shA[k];
+  }
+  __syncthreads();
+  const uint32_t cnt = a.n - i0 < 128u ? a.n - i0 : 128u;  // splats of this block
+  const uint32_t nP = cnt * STRIDE, nS = cnt * SHN;
+  const size_t pBase = (size_t)i0 * STRIDE, sBase = (size_t)i0 * SHN;
+  if (a.gradF) {
+    for (uint32_t e = t; e < nP; e += 128) a.gradF[pBase + e] = s_g[(e / STRIDE) * GROW + e % STRIDE];
+    for (uint32_t e = t; e < nS; e += 128) a.shGrad[sBase + e] = s_sh[(e / SHD) * SROW + e % SHD];
+  }
+  if (!a.doAdam) return;
+  const AdamHP& h = *a.hp;
+  for (uint32_t e = t; e < nP; e += 128) {
+    const int slot = (int)(e % STRIDE);
+    float p = a.params[pBase + e], m = a.m[pBase + e], vv = a.v[pBase + e];
+    adamParam(h, slot, p, s_g[(e / STRIDE) * GROW + slot], m, vv);
+    a.params[pBase + e] = p;
+    a.m[pBase + e] = m;
+    a.v[pBase + e] = vv;
+  }
+  for (uint32_t e = t; e < nS; e += 128) {
+    float g = s_sh[(e / SHD) * SROW + e % SHD];
+    if (!(fabsf(g) < 1e18f)) g = 0.0f;
+    const float mk = h.b1 * a.shM[sBase + e] + (1.0f - h.b1) * g;
+    const float vk = h.b2 * a.shV[sBase + e] + (1.0f - h.b2) * g * g;
+    a.shM[sBase + e] = mk;
+    a.shV[sBase + e] = vk;
+    const float mh = mk / h.bc1, vh = vk / h.bc2;
+    a.sh[sBase + e] = a.sh[sBase + e] - h.shLr * mh / (sqrtf(vh) + h.eps);
   }
 }
 
 void launch_chain_adam(const ChainArgs& a, int deg, cudaStream_t s) {
-  const unsigned grid = (a.n + 127) / 128;
-  if (grid == 0) return;
-  if (a.V > 1) launch_chain_t<true>(a, deg, grid, s);
-  else launch_chain_t<false>(a, deg, grid, s);
+  const unsigned blocks = (a.n + 127) / 128;
+  if (blocks == 0) return;
+  const unsigned g1 = blocks * (unsigned)a.V;
+  switch (deg) {
+    case 0: k_chain_view<0><<<g1, 128, 0, s>>>(a); k_chain_adam<0><<<blocks, 128, 0, s>>>(a); break;
+    case 1: k_chain_view<1><<<g1, 128, 0, s>>>(a); k_chain_adam<1><<<blocks, 128, 0, s>>>(a); break;
+    case 2: k_chain_view<2><<<g1, 128, 0, s>>>(a); k_chain_adam<2><<<blocks, 128, 0, s>>>(a); break;
+    default: k_chain_view<3><<<g1, 128, 0, s>>>(a); k_chain_adam<3><<<blocks, 128, 0, s>>>(a); break;
+  }
 }
 
 }  // namespace gs

@@ -126,6 +126,10 @@ struct AdamHP {
   float b1, b2, eps, bc1, bc2, minLS, maxLS, maxLogit, reg, shLr;
 };
 
+// floats per (view, splat) chain result: 14 parameter gradients, gated
+// colour gradient (3), view direction (3)
+constexpr int VIEWGRAD_STRIDE = 20;
+
 struct ChainArgs {
   uint32_t n;
   int V;
@@ -134,6 +138,7 @@ struct ChainArgs {
   float* sh;
   int32_t* gradP;
   const uint2* rect;
+  float* viewGrad;         // V * n * VIEWGRAD_STRIDE: per-(view, splat) chain results
   float anisoReg;
   int32_t* gradCam;
   float* gradF;            // optional readout (n * 16)

@@ -79,6 +79,7 @@ struct gs_trainer {
   uint32_t *counts = nullptr, *offsets = nullptr;
   unsigned long long* liveMask = nullptr;
   float4* cullRecs = nullptr;
+  float* viewGrad = nullptr;
   int32_t* gradP = nullptr;
   int32_t* diffGrid = nullptr;
   uint32_t* tileCnt = nullptr;
@@ -383,6 +384,7 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   GS_AL(h->offsets, (size_t)B * cap);
   GS_AL(h->liveMask, (size_t)B * cap);
   GS_AL(h->cullRecs, (size_t)B * cap);
+  GS_AL(h->viewGrad, (size_t)B * cap * VIEWGRAD_STRIDE);
   GS_AL(h->gradP, (size_t)B * cap * GP_STRIDE);
   // (tx+1)(ty+1) = tiles + tx + ty + 1 <= 3 * maxTiles + 1 for any view of at most maxTiles tiles
   GS_AL(h->diffGrid, (size_t)B * (3 * (size_t)h->maxTiles + 1));
@@ -667,9 +669,9 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   if (cull) launch_ranges_from_keys(h->keys[passes & 1], totalEntries, totalTiles, h->ranges, s);
   // kernels: project, tile counts + finish, presort (histogram + passes),
   // entry counts, 3 scan kernels, entry keys, tile sort (histogram +
-  // passes), [ranges from keys], [work order], raster, [chain+Adam]
+  // passes), [ranges from keys], [work order], raster, [chain per view, sum + Adam]
   h->lastLaunches = 3u + 1u + (uint32_t)pr.passes + 1u + 3u + 1u + 1u + (uint32_t)passes + (cull ? 1u : 0u) +
-                    (h->o.persistent ? 1u : 0u) + 1u + (sh.chain ? 1u : 0u);
+                    (h->o.persistent ? 1u : 0u) + 1u + (sh.chain ? 2u : 0u);
   const uint32_t* sortedIds = h->vals[passes & 1];
 
   const bool persistent = h->o.persistent != 0;
@@ -715,6 +717,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
     c.sh = h->K ? h->sh : nullptr;
     c.gradP = h->gradP;
     c.rect = h->rect;
+    c.viewGrad = h->viewGrad;
     c.anisoReg = h->o.anisoReg;
     c.gradCam = h->gradCam;
     c.gradF = sh.grads ? h->gradFOut : nullptr;

@@ -9,7 +9,8 @@ import ctypes as C
 import os
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG_DIR, "libsplat_b200.so")
+# SPLAT_B200_LIB: load a library built elsewhere (default: the in-tree build)
+LIB_PATH = os.environ.get("SPLAT_B200_LIB") or os.path.join(PKG_DIR, "libsplat_b200.so")
 HEADER = os.path.join(os.path.dirname(PKG_DIR), "include", "splat_b200.h")
 
 GS_OK = 0
