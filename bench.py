@@ -351,19 +351,27 @@ def run_ours(args):
     N.check(L.gs_profile_read(h, ms4, cnt4), h)
     N.check(L.gs_profile(h, 0), h)
     phase = {nm: ms4[i] / max(1, cnt4[i]) for i, nm in enumerate(["project_bin", "sort", "raster", "chain_adam"])}
-    # pairs of one batch (for the raster roofline): sum of per-pixel end indices
-    pairs = 0
-    for k in range(prof_steps):
-        cs = batch_cams(k)
-        arr = (C.c_uint32 * len(cs))(*cs)
-        N.check(L.gs_raster_pass(h, arr, len(cs), 3), h)
-        for v, ci in enumerate(cs):
-            w, hh = allcams[ci]["w"], allcams[ci]["h"]
-            end = np.zeros(w * hh, np.uint32)
-            N.check(L.gs_debug_pixels(h, v, None, None, N.ptr(end, C.c_uint32)), h)
-            pairs += int(end.astype(np.uint64).sum())
-            N.check(L.gs_debug_gradp(h, v, None, 1), h)   # leave no gradients behind
-    pairs_per_launch = pairs / prof_steps
+    # pixel-entry pairs of one batch (the raster roofline's work unit): the sum
+    # of per-pixel end indices.  The algorithmic count P is taken on the
+    # reference's full rectangle tile lists (tile cull off); the culled lists
+    # the step actually walks give the executed count beside it.
+    def count_pairs(cull):
+        N.check(L.gs_set_tile_cull(h, cull), h)
+        total = 0
+        for k in range(prof_steps):
+            cs = batch_cams(k)
+            arr = (C.c_uint32 * len(cs))(*cs)
+            N.check(L.gs_raster_pass(h, arr, len(cs), 3), h)
+            for v, ci in enumerate(cs):
+                w, hh = allcams[ci]["w"], allcams[ci]["h"]
+                end = np.zeros(w * hh, np.uint32)
+                N.check(L.gs_debug_pixels(h, v, None, None, N.ptr(end, C.c_uint32)), h)
+                total += int(end.astype(np.uint64).sum())
+                N.check(L.gs_debug_gradp(h, v, None, 1), h)   # leave no gradients behind
+        return total / prof_steps
+    pairs_exec = count_pairs(1)
+    pairs_per_launch = count_pairs(0)
+    N.check(L.gs_set_tile_cull(h, 1), h)
     peak = C.c_double()
     N.check(L.gs_probe_fp32_peak(local, C.byref(peak)), None)
     raster_ms = phase["raster"]
@@ -392,11 +400,14 @@ def run_ours(args):
                 "gpu_launches": None,
                 "phases_ms_per_step": phase,
                 "pairs_per_step": pairs_per_launch,
+                "pairs_executed_per_step": pairs_exec,
                 "roofline": {"bound": "fp32", "kernel": "raster (fused forward + loss + backward)",
                              "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                              "frac": achieved / peak.value if peak.value else None, "traffic": None,
                              "peak_source": "gs_probe_fp32_peak FFMA kernel on this GPU (measured)",
-                             "work": f"{FLOP_PER_PAIR} flop per evaluated pixel-entry pair"},
+                             "work": f"{FLOP_PER_PAIR} flop per pixel-entry pair P of the reference's tile lists "
+                                     "(pairs up to each pixel's termination index); the step walks culled lists "
+                                     "with pairs_executed_per_step of them"},
                 "clocks": clocks,
                 "cpu_baseline": cpu}
         line["gpu_launches"] = batch_launches * args.steps

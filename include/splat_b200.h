@@ -216,6 +216,10 @@ GS_API int gs_sort_entries_static(uint32_t* keys, uint32_t* vals, uint32_t n, ui
 GS_API int gs_autotune(gs_trainer* h, const uint32_t* ci, uint32_t nviews, int32_t reps, int32_t* bestTile,
                        int32_t* bestDepth, float* msOut);
 GS_API int gs_set_raster_config(gs_trainer* h, int32_t tile, int32_t batchDepth);
+/* Switch the tile cull (gs_options.tileCull) for later steps: 0 gives the
+ * reference's full rectangle lists (used to count the reference's pixel-entry
+ * pairs); results are identical either way. */
+GS_API int gs_set_tile_cull(gs_trainer* h, int32_t enable);
 
 /* ---- introspection of the most recent raster (parity checks) ----
  * gs_raster_pass runs project -> bin -> raster (no chain, no Adam) on views

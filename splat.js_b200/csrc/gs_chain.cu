@@ -231,7 +231,7 @@ __device__ __forceinline__ void adamParam(const AdamHP& h, int slot, float& p, f
 }
 
 #ifndef GS_CHAIN_MIN_BLOCKS
-#define GS_CHAIN_MIN_BLOCKS 1  // resident 128-thread blocks per SM the register allocation must allow
+#define GS_CHAIN_MIN_BLOCKS 5  // resident 128-thread blocks per SM the register allocation must allow
 #endif
 
 // Pass 1: one thread per (view, splat).  Blocks are ordered splat block major,

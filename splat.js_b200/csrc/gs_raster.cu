@@ -96,11 +96,11 @@ __device__ __forceinline__ uint32_t warp_block_mask(const float4 cq, float mx, f
 }
 
 #ifndef GS_RASTER16_MIN_BLOCKS
-#define GS_RASTER16_MIN_BLOCKS 1  // resident 16x16-tile blocks per SM the register allocation must allow
+#define GS_RASTER16_MIN_BLOCKS 5  // resident 16x16-tile blocks per SM the register allocation must allow
 #endif
 // TILE x TILE pixels per CTA, one per thread; warps cover 8x4 blocks.
 template <int TILE, int BATCH, bool FWD, bool BWD, bool STORED>
-__global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOCKS : 1) k_raster(RasterArgs a) {
+__global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOCKS : TILE == 8 ? 16 : 1) k_raster(RasterArgs a) {
   constexpr int RT = TILE;
   constexpr int RTHREADS = TILE * TILE;
   constexpr int NW = RTHREADS / 32;  // warps

@@ -46,6 +46,7 @@ struct Shape {
   int variant;
   int tile;       // raster tile edge
   int depth;      // splat-batch depth
+  int cull;       // tile lists culled by the ellipse/tile test
   bool operator<(const Shape& o) const { return std::memcmp(this, &o, sizeof(Shape)) < 0; }
 };
 
@@ -620,7 +621,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   launch_radix_sort(pr, s);
   const uint32_t* sortedSlots = h->pvals[pr.passes & 1];
 
-  const bool cull = h->o.tileCull != 0;
+  const bool cull = sh.cull != 0;
   ExpandArgs ea{};
   ea.n = sh.n;
   ea.V = V;
@@ -840,6 +841,7 @@ static Shape make_shape(gs_trainer* h, const DevCam* views, int V, int mode, int
   sh.variant = h->o.backwardVariant;
   sh.tile = h->tile;
   sh.depth = h->o.batchDepth;
+  sh.cull = h->o.tileCull;
   return sh;
 }
 
@@ -1150,6 +1152,13 @@ int gs_set_raster_config(gs_trainer* h, int32_t tile, int32_t batchDepth) {
     return fail(h, GS_E_INVALID, "batchDepth must be 64, 128 or 256");
   h->tile = tile;
   h->o.batchDepth = batchDepth;
+  return GS_OK;
+}
+
+int gs_set_tile_cull(gs_trainer* h, int32_t enable) {
+  if (!h) return GS_E_INVALID;
+  if (enable != 0 && enable != 1) return fail(h, GS_E_INVALID, "tileCull must be 0 or 1");
+  h->o.tileCull = enable;
   return GS_OK;
 }
 

@@ -103,6 +103,7 @@ def lib():
         "gs_sort_entries_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]),
         "gs_autotune": (C.c_int, [H, u32p, C.c_uint32, C.c_int32, i32p, i32p, f32p]),
         "gs_set_raster_config": (C.c_int, [H, C.c_int32, C.c_int32]),
+        "gs_set_tile_cull": (C.c_int, [H, C.c_int32]),
         "gs_raster_pass": (C.c_int, [H, u32p, C.c_uint32, C.c_int32]),
         "gs_debug_records": (C.c_int, [H, C.c_uint32, f32p, u32p]),
         "gs_debug_binning": (C.c_int, [H, C.c_uint32, u32p, u32p, u32p, C.c_uint64, u64p]),
