@@ -193,12 +193,18 @@ GS_API int gs_profile_read(gs_trainer* h, double ms[4], uint32_t launches[4]);
  * the peak the raster kernels' roofline is quoted against. */
 GS_API int gs_probe_fp32_peak(int32_t device, double* tflops);
 
-/* ---- allocation-free entry sort (no reference counterpart) ----
+/* ---- allocation-free entry sort (no counterpart in the reference) ----
+ * For callers that cannot call cudaMalloc: code whose device memory is owned
+ * by another runtime's pool (a host application or binding that forbids
+ * foreign allocations), and code on a path where an allocation -- which may
+ * synchronise the device -- is not allowed.
  * Stable LSD radix sort of n (key, value) pairs held in device memory, in
  * place, on key bits [0, keyBits): the sort that orders the trainer's
  * (tile id, splat id) entries, run with its scratch in statically sized
  * device arrays instead of buffers the trainer allocates, so the call
- * allocates no memory.  n above GS_STATIC_SORT_MAX returns GS_E_LIMIT.
+ * allocates nothing.  Every GPU that loads the library holds that scratch
+ * (about 8.5 MB) until the process exits.  n above GS_STATIC_SORT_MAX
+ * returns GS_E_LIMIT.
  * keys/vals: device pointers on the current device; stream may be NULL.
  * The first call on a device sets the scratch up (symbol lookup and a
  * synchronous clear), so make it before any stream capture.  The call

@@ -7,9 +7,11 @@
 // It restates, function by function, the WGSL kernels of the reference
 // (src/gs/shaders.js) and the host logic of src/gs/trainer.js.  Every
 // function cites the lines it follows.  The reference itself only runs
-// under WebGPU (a graphics API), so its GPU output cannot be produced here;
-// oracle/wgsl_ref.py compiles the reference's own WGSL as C++ into
-// oracle/_ref/ and tests/golden/ holds vectors made from it.
+// under WebGPU (a graphics API), which is unavailable on this box, and it
+// stores no golden vectors, so parity with the reference's own output is
+// UNPINNED.  What pins this restatement is the reference's own check of its
+// backward (src/gs/gradcheck.js): the same 160-splat rig and central finite
+// differences of the FP64 loss (tests/test_oracle_pin.py).
 //
 // Two instantiations:
 //   T = float   the FP32 path.  Its evaluation order is fixed exactly (see

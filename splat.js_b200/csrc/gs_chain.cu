@@ -374,23 +374,56 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
   }
   if (!a.doAdam) return;
   const AdamHP& h = *a.hp;
-  for (uint32_t e = t; e < nP; e += 128) {
-    const int slot = (int)(e % STRIDE);
-    float p = a.params[pBase + e], m = a.m[pBase + e], vv = a.v[pBase + e];
-    adamParam(h, slot, p, s_g[(e / STRIDE) * GROW + slot], m, vv);
-    a.params[pBase + e] = p;
-    a.m[pBase + e] = m;
-    a.v[pBase + e] = vv;
+  // four elements per thread in flight: loads first, then the updates
+  constexpr uint32_t U = 4;
+  {
+    float* __restrict__ Pp = a.params + pBase;
+    float* __restrict__ Pm = a.m + pBase;
+    float* __restrict__ Pv = a.v + pBase;
+    const int slot = t % STRIDE;  // 128 is a multiple of the stride: one slot per thread
+    for (uint32_t e0 = t; e0 < nP; e0 += 128 * U) {
+      float p[U], m[U], vv[U];
+#pragma unroll
+      for (uint32_t u = 0; u < U; ++u) {
+        const uint32_t e = e0 + 128 * u;
+        if (e < nP) { p[u] = Pp[e]; m[u] = Pm[e]; vv[u] = Pv[e]; }
+      }
+#pragma unroll
+      for (uint32_t u = 0; u < U; ++u) {
+        const uint32_t e = e0 + 128 * u;
+        if (e < nP) {
+          adamParam(h, slot, p[u], s_g[(e / STRIDE) * GROW + slot], m[u], vv[u]);
+          Pp[e] = p[u]; Pm[e] = m[u]; Pv[e] = vv[u];
+        }
+      }
+    }
   }
-  for (uint32_t e = t; e < nS; e += 128) {
-    float g = s_sh[(e / SHD) * SROW + e % SHD];
-    if (!(fabsf(g) < 1e18f)) g = 0.0f;
-    const float mk = h.b1 * a.shM[sBase + e] + (1.0f - h.b1) * g;
-    const float vk = h.b2 * a.shV[sBase + e] + (1.0f - h.b2) * g * g;
-    a.shM[sBase + e] = mk;
-    a.shV[sBase + e] = vk;
-    const float mh = mk / h.bc1, vh = vk / h.bc2;
-    a.sh[sBase + e] = a.sh[sBase + e] - h.shLr * mh / (sqrtf(vh) + h.eps);
+  if (SHN > 0) {
+    float* __restrict__ Sw = a.sh + sBase;
+    float* __restrict__ Sm = a.shM + sBase;
+    float* __restrict__ Sv = a.shV + sBase;
+    for (uint32_t e0 = t; e0 < nS; e0 += 128 * U) {
+      float w[U], m[U], vv[U];
+#pragma unroll
+      for (uint32_t u = 0; u < U; ++u) {
+        const uint32_t e = e0 + 128 * u;
+        if (e < nS) { w[u] = Sw[e]; m[u] = Sm[e]; vv[u] = Sv[e]; }
+      }
+#pragma unroll
+      for (uint32_t u = 0; u < U; ++u) {
+        const uint32_t e = e0 + 128 * u;
+        if (e < nS) {
+          float g = s_sh[(e / SHD) * SROW + e % SHD];
+          if (!(fabsf(g) < 1e18f)) g = 0.0f;
+          const float mk = h.b1 * m[u] + (1.0f - h.b1) * g;
+          const float vk = h.b2 * vv[u] + (1.0f - h.b2) * g * g;
+          const float mh = mk / h.bc1, vh = vk / h.bc2;
+          Sm[e] = mk;
+          Sv[e] = vk;
+          Sw[e] = w[u] - h.shLr * mh / (sqrtf(vh) + h.eps);
+        }
+      }
+    }
   }
 }
 

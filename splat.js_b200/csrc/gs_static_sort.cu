@@ -6,7 +6,12 @@
 // buffers the trainer allocates at set-up.  This entry point runs the same
 // kernels with all of that scratch in file-scope __device__ arrays sized for
 // at most GS_STATIC_SORT_MAX entries, so a call allocates no device or host
-// memory: it can be used where an allocator must not be entered.
+// memory.  It serves callers that cannot call cudaMalloc: code whose device
+// memory is owned by another runtime's pool, and code on a path where an
+// allocation (which may synchronise the device) is not allowed.  Every GPU
+// that loads the library holds the arrays (about 8.5 MB) until exit.  In host
+// code the arrays' names are host-side stand-ins, never device addresses:
+// only the addresses cudaGetSymbolAddress returns are passed to kernels.
 //
 // Set-up: the first call on a device resolves the arrays' addresses with
 // cudaGetSymbolAddress (with that device current) and clears the look-back

@@ -1,6 +1,11 @@
 """The allocation-free entry sort (gs_sort_entries_static) against the
 trainer's own binning (gs_debug_binning), through the C ABI (B200 required).
 
+The entry point exists for callers that cannot call cudaMalloc (their device
+memory belongs to another runtime's pool, or an allocation's implicit
+synchronisation is not allowed on their path); its scratch is a static
+device array, so these checks also run it twice on the same scratch.
+
 The input is built the way the trainer builds its entries: splats in
 (depth bits, id) order, each expanding to the tiles of its rectangle in row
 order, key = tile id, value = splat id.  A stable sort on the tile id must
