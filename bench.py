@@ -222,19 +222,44 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
-# GPU arm
+# Rank plumbing (one process per GPU; replicas, no data-path collective)
 # ---------------------------------------------------------------------------
-def run_ours(args):
-    import torch
+def init_ranks(backend="nccl", timeout_s=300):
+    """(rank, world, local rank, torch.distributed or None) from the launcher's
+    environment; a process group only when WORLD_SIZE > 1."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+    return rank, world, local, dist
+
+
+def max_over_ranks(ms, dist, device):
+    """The slowest rank's time: every rank returns the same value."""
+    if not dist:
+        return ms
+    import torch
+    tt = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def job_rate(units_per_step, steps, world, ms):
+    """Whole-job throughput: units every rank processed / the slowest rank's time."""
+    return units_per_step * steps * world / (ms / 1e3)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    rank, world, local, dist = init_ranks("nccl")
+    torch.cuda.set_device(local)
 
     from splat_b200 import native as N
     from splat_b200 import scene
@@ -287,12 +312,8 @@ def run_ours(args):
             fn(k)
         e1.record(stream)
         barrier()
-        ms = e0.elapsed_time(e1)
-        if dist:
-            tt = torch.tensor([ms], device=f"cuda:{local}")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms = float(tt.item())
-        return ms, views_per_step * steps * world / (ms / 1e3)
+        ms = max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{local}")
+        return ms, job_rate(views_per_step, steps, world, ms)
 
     arrs = {}
 
