@@ -455,51 +455,69 @@ inline Splat2D<T> splat2D(const T* pr) {
   return s;
 }
 
-// Tile cull of the B200 library (no reference counterpart): keeps a (splat,
-// tile) entry only when some pixel centre of the tile can pass the
-// rasteriser's test e <= eCut and w exp(-e) >= aMin.  The exact minimum of
-// e = hA dx^2 + B dx dy + hC dy^2 over the tile's pixel-centre rectangle is
-// taken in double (edge minima at dy = kx dx, dx = ky dy, clamped) and
-// compared with min(eCut, eA) (eA = log_f(w / aMin)) plus margins for the
-// FP32 evaluation; the library runs the same sequence, so both keep the same
-// entries.  Culled entries contribute to no pixel.  A single-tile rectangle
-// keeps its tile untested.
-struct CullSplat {
-  float mx, my, hA, B, hC, eA;
-  double kx, ky;
-};
-
-inline CullSplat cullPrep(float mx, float my, float hA, float B, float hC, float w, float aMin) {
-  CullSplat s;
-  s.mx = mx; s.my = my; s.hA = hA; s.B = B; s.hC = hC;
-  s.eA = log_f(w / aMin);
-  s.kx = -(double)B / (2.0 * (double)hC);
-  s.ky = -(double)B / (2.0 * (double)hA);
-  return s;
+// Tile cull of the B200 library (no reference counterpart).  Keeps a
+// (splat, tile) entry only when some pixel centre of the tile can pass the
+// rasteriser's test e <= eCut and w exp(-e) >= aMin; the library runs the
+// same sequence (cullParams / bandInterval / tileLive), so both keep the same
+// entries.  Culled entries contribute to no pixel.
+//
+// Per splat and view, completing the square in dx: a pixel (dx, dy) with
+// exact exponent e <= t satisfies |dx - kA dy| <= sqrt(p - q dy^2), with
+// kA = -B/(2 hA), p = t/hA, q = (4 hA hC - B^2)/(4 hA^2), and t =
+// min(eCut, ln(w/aMin)) plus margins for the FP32 evaluation.  Computed in
+// double; p rounded up, q down, kA to nearest.  p = +inf: keep everything.
+inline float f32_up(double x) {
+  float f = (float)x;
+  if ((double)f < x) f = std::nextafter(f, INFINITY);
+  return f;
 }
-
-inline bool tileLive(const CullSplat& s, float eCut, int tx, int ty, int tile, int W, int H) {
-  if (!(s.hA > 0.0f) || !(s.hC > 0.0f)) return true;
-  const int xe = std::min(tx * tile + tile, W), ye = std::min(ty * tile + tile, H);
-  const double X0 = ((double)(tx * tile) + 0.5) - (double)s.mx;
-  const double X1 = ((double)(xe - 1) + 0.5) - (double)s.mx;
-  const double Y0 = ((double)(ty * tile) + 0.5) - (double)s.my;
-  const double Y1 = ((double)(ye - 1) + 0.5) - (double)s.my;
-  const double a = s.hA, b = s.B, c = s.hC;
-  double emin = 0.0;
-  if (!(X0 <= 0.0 && X1 >= 0.0 && Y0 <= 0.0 && Y1 >= 0.0)) {
-    const double dy0 = std::fmin(std::fmax(s.kx * X0, Y0), Y1), dy1 = std::fmin(std::fmax(s.kx * X1, Y0), Y1);
-    const double dx0 = std::fmin(std::fmax(s.ky * Y0, X0), X1), dx1 = std::fmin(std::fmax(s.ky * Y1, X0), X1);
-    const double e0 = (a * X0) * X0 + (b * X0) * dy0 + (c * dy0) * dy0;
-    const double e1 = (a * X1) * X1 + (b * X1) * dy1 + (c * dy1) * dy1;
-    const double e2 = (a * dx0) * dx0 + (b * dx0) * Y0 + (c * Y0) * Y0;
-    const double e3 = (a * dx1) * dx1 + (b * dx1) * Y1 + (c * Y1) * Y1;
-    emin = std::fmin(std::fmin(e0, e1), std::fmin(e2, e3));
+inline float f32_down(double x) {
+  float f = (float)x;
+  if ((double)f > x) f = std::nextafter(f, -INFINITY);
+  return f;
+}
+struct CullParams { float p, q, kA; };
+inline CullParams cullParams(float mx, float my, float hA, float B, float hC, float w, float aMin, float eCut,
+                             int x0, int x1, int y0, int y1, int tile) {
+  CullParams c{INFINITY, 0.0f, 0.0f};
+  const double A = hA, Bq = B, Cq = hC;
+  const double det = 4.0 * A * Cq - Bq * Bq;
+  if (A > 0.0 && Cq > 0.0 && det > 0.0) {
+    const double dmx = mx, dmy = my, T = tile;
+    const double ax = std::fmax(dmx - (double)x0 * T, (double)(x1 + 1) * T - dmx);
+    const double ay = std::fmax(dmy - (double)y0 * T, (double)(y1 + 1) * T - dmy);
+    const double smax = (A * ax) * ax + (std::fabs(Bq) * ax) * ay + (Cq * ay) * ay;
+    const double eA = (double)log_f(w / aMin);
+    const double tmax = std::fmin((double)eCut, eA + 1.0e-5) + 2.0e-6 * smax + 1.0e-6;
+    c.p = f32_up(tmax / A);
+    c.q = f32_down(det / (4.0 * A * A));
+    c.kA = (float)(-Bq / (2.0 * A));
   }
-  const double ax = std::fmax(-X0, X1), ay = std::fmax(-Y0, Y1);
-  const double smax = (a * ax) * ax + (std::fabs(b) * ax) * ay + (c * ay) * ay;
-  const double thr = std::fmin((double)eCut, (double)s.eA + 1.0e-5) + 2.0e-6 * smax + 1.0e-6;
-  return emin <= thr;
+  return c;
+}
+// dx interval of the reachable pixels of the band of rows dy in [Y0, Y1]
+// (FP32, with slack for this evaluation); false: band unreachable.
+inline bool bandInterval(const CullParams& c, float Y0, float Y1, float& xl, float& xr) {
+  float d = Y0 > 0.0f ? Y0 : (Y1 < 0.0f ? -Y1 : 0.0f);
+  d = std::fmax(d - (1.0e-3f + 1.0e-6f * d), 0.0f);
+  const float rad2 = std::fma(-c.q, d * d, c.p) + 1.0e-5f * c.p;
+  if (!(rad2 >= 0.0f)) return false;
+  const float r = std::sqrt(rad2) * 1.00001f;
+  const float c0 = c.kA * Y0, c1 = c.kA * Y1;
+  const float cl = std::fmin(c0, c1), ch = std::fmax(c0, c1);
+  const float sl = 4.0e-3f * (1.0f + std::fabs(c.kA)) + 1.0e-5f * (std::fabs(cl) + std::fabs(ch) + r);
+  xl = (cl - r) - sl;
+  xr = (ch + r) + sl;
+  return true;
+}
+inline bool tileLive(const CullParams& c, float mx, float my, int tx, int ty, int tile, int W, int H) {
+  if (!(c.p < 3.0e38f)) return true;
+  const int xe = std::min(tx * tile + tile, W), ye = std::min(ty * tile + tile, H);
+  float xl, xr;
+  if (!bandInterval(c, ((float)(ty * tile) + 0.5f) - my, ((float)(ye - 1) + 0.5f) - my, xl, xr)) return false;
+  const float X0 = ((float)(tx * tile) + 0.5f) - mx;
+  const float X1 = ((float)(xe - 1) + 0.5f) - mx;
+  return X1 >= xl && X0 <= xr;
 }
 
 template <class T>
@@ -515,16 +533,18 @@ inline Bins binTiles(const Opts& o, const Cam& c, const T* proj, uint32_t n) {
     TileRect r = tileRect<T>(c, o.tile, pr[0], pr[1], pr[15]);
     const float depth = (float)pr[2];
     const bool test = o.tileCull && !(r.x0 == r.x1 && r.y0 == r.y1);
-    CullSplat cs{};
+    CullParams cp{INFINITY, 0.0f, 0.0f};
+    float cmx = 0.0f, cmy = 0.0f;
     if (test) {
       const Splat2D<T> s2 = splat2D<T>(pr);
-      cs = cullPrep((float)s2.mx, (float)s2.my, (float)(T(0.5) * s2.cA), (float)s2.cB, (float)(T(0.5) * s2.cC),
-                    (float)s2.w, o.aMin);
+      cmx = (float)s2.mx; cmy = (float)s2.my;
+      cp = cullParams(cmx, cmy, (float)(T(0.5) * s2.cA), (float)s2.cB, (float)(T(0.5) * s2.cC), (float)s2.w, o.aMin,
+                      o.eCut, r.x0, r.x1, r.y0, r.y1, o.tile);
     }
     for (int y = r.y0; y <= r.y1; ++y)
       for (int x = r.x0; x <= r.x1; ++x) {
         b.cnt[y * tx + x]++;  // the budget counts every rectangle tile
-        if (test && !tileLive(cs, o.eCut, x, y, o.tile, c.W, c.H)) continue;
+        if (test && !tileLive(cp, cmx, cmy, x, y, o.tile, c.W, c.H)) continue;
         lists[y * tx + x].push_back({fbits(depth), i});
       }
   }

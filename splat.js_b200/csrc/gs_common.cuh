@@ -89,56 +89,73 @@ __device__ __forceinline__ float glog(float x) {
   return __fmaf_rn(fe, 0.693145751953125f, __fmaf_rn(fe, 1.42860676533018700e-6f, lm));
 }
 
-// Tile cull: can any pixel centre of tile (tx, ty) pass the rasteriser's
-// test (e <= eCut and alpha = w exp(-e) >= aMin) for the splat with mean
-// (mx, my) and conic halves (hA, B, hC)?  The exact minimum of
-// e = hA dx^2 + B dx dy + hC dy^2 over the rectangle of the tile's pixel
-// centres (clipped to the image) is computed in double -- on an edge dx = X
-// the minimum lies at dy = kx X clamped to the edge, kx = -B / (2 hC), and
-// likewise with ky = -B / (2 hA) -- and compared with min(eCut, eA) plus
-// margins that cover the rasteriser's FP32 evaluation (a few ulp of the
-// largest term, bounded by smax) and the canonical log (eA = glog(w / aMin)).
-// Every pixel that passes the FP32 test lies in a tile that passes this one,
-// so dropping the other entries changes no pixel.  The oracle runs the same
-// double-precision sequence, so both keep the same entries.  A splat whose
-// rectangle is a single tile keeps it without the test.
-struct CullSplat {
-  float mx, my, hA, B, hC, eA;
-  double kx, ky;
-};
-
-__device__ __forceinline__ CullSplat cullPrep(float mx, float my, float hA, float B, float hC, float w, float aMin) {
-  CullSplat s;
-  s.mx = mx; s.my = my; s.hA = hA; s.B = B; s.hC = hC;
-  s.eA = glog(w / aMin);
-  s.kx = -(double)B / (2.0 * (double)hC);
-  s.ky = -(double)B / (2.0 * (double)hA);
-  return s;
+// Cull parameters of one splat in one view.  Completing the square in dx, a
+// pixel (dx, dy) (offsets from the mean) with exact exponent
+// e = hA dx^2 + B dx dy + hC dy^2 <= t satisfies
+//   |dx - kA dy| <= sqrt(p - q dy^2),  kA = -B / (2 hA), p = t / hA,
+//   q = (4 hA hC - B^2) / (4 hA^2).
+// t is the largest exponent the rasteriser can accept, min(eCut, ln(w/aMin)),
+// plus margins for its FP32 evaluation (2e-6 of the largest term over the
+// splat's tile rectangle, which bounds a few ulp of every term) and for the
+// canonical log (1e-5).  Computed in double; p is rounded up, q down and kA
+// to nearest, so the bound stays conservative.  (p, q, kA) = (+inf, 0, 0)
+// marks a degenerate conic: every pixel is kept.  The oracle repeats this
+// sequence exactly.
+__device__ __forceinline__ float4 cullParams(float mx, float my, float hA, float B, float hC, float w, float aMin,
+                                             float eCut, uint32_t x0, uint32_t x1, uint32_t y0, uint32_t y1,
+                                             int tile) {
+  float4 cq = make_float4(__int_as_float(0x7F800000), 0.0f, 0.0f, 0.0f);
+  const double A = (double)hA, Bq = (double)B, Cq = (double)hC;
+  const double det = 4.0 * A * Cq - Bq * Bq;
+  if (A > 0.0 && Cq > 0.0 && det > 0.0) {
+    const double dmx = (double)mx, dmy = (double)my, T = (double)tile;
+    const double ax = fmax(dmx - (double)x0 * T, (double)(x1 + 1) * T - dmx);
+    const double ay = fmax(dmy - (double)y0 * T, (double)(y1 + 1) * T - dmy);
+    const double smax = (A * ax) * ax + (fabs(Bq) * ax) * ay + (Cq * ay) * ay;
+    const double eA = (double)glog(w / aMin);
+    const double tmax = fmin((double)eCut, eA + 1.0e-5) + 2.0e-6 * smax + 1.0e-6;
+    cq.x = __double2float_ru(tmax / A);
+    cq.y = __double2float_rd(det / (4.0 * A * A));
+    cq.z = __double2float_rn(-Bq / (2.0 * A));
+  }
+  return cq;
 }
 
-__device__ __forceinline__ bool tileLive(const CullSplat& s, float eCut, int tx, int ty, int tile, int W, int H) {
-  if (!(s.hA > 0.0f) || !(s.hC > 0.0f)) return true;
+// The dx interval [xl, xr] that holds every reachable pixel of the band of
+// pixel-centre rows with dy in [Y0, Y1]: |dx - kA dy| <= sqrt(p - q dmin^2),
+// dmin the band's smallest |dy|.  Slack covers this FP32 evaluation (the
+// rounding of Y0/Y1 and of the products).  false: the band is unreachable.
+// p = +inf never gets here (callers keep everything).
+__device__ __forceinline__ bool bandInterval(const float4 cq, float Y0, float Y1, float& xl, float& xr) {
+  const float p = cq.x, q = cq.y, kA = cq.z;
+  float d = Y0 > 0.0f ? Y0 : (Y1 < 0.0f ? -Y1 : 0.0f);
+  d = fmaxf(d - (1.0e-3f + 1.0e-6f * d), 0.0f);
+  const float rad2 = __fmaf_rn(-q, d * d, p) + 1.0e-5f * p;
+  if (!(rad2 >= 0.0f)) return false;
+  const float r = sqrtf(rad2) * 1.00001f;
+  const float c0 = kA * Y0, c1 = kA * Y1;
+  const float cl = fminf(c0, c1), ch = fmaxf(c0, c1);
+  const float sl = 4.0e-3f * (1.0f + fabsf(kA)) + 1.0e-5f * (fabsf(cl) + fabsf(ch) + r);
+  xl = (cl - r) - sl;
+  xr = (ch + r) + sl;
+  return true;
+}
+
+// Tile cull: can any pixel centre of tile (tx, ty) (clipped to the W x H
+// image) be reachable?  A (splat, tile) entry that fails cannot composite
+// into any pixel of the tile, so dropping it changes no image, loss or
+// gradient.  The oracle runs the same FP32 sequence, so both keep the same
+// entries.
+__device__ __forceinline__ bool tileLive(const float4 cq, float mx, float my, int tx, int ty, int tile, int W,
+                                         int H) {
+  if (!(cq.x < 3.0e38f)) return true;
   const int xe = tx * tile + tile < W ? tx * tile + tile : W;
   const int ye = ty * tile + tile < H ? ty * tile + tile : H;
-  const double X0 = ((double)(tx * tile) + 0.5) - (double)s.mx;
-  const double X1 = ((double)(xe - 1) + 0.5) - (double)s.mx;
-  const double Y0 = ((double)(ty * tile) + 0.5) - (double)s.my;
-  const double Y1 = ((double)(ye - 1) + 0.5) - (double)s.my;
-  const double a = (double)s.hA, b = (double)s.B, c = (double)s.hC;
-  double emin = 0.0;
-  if (!(X0 <= 0.0 && X1 >= 0.0 && Y0 <= 0.0 && Y1 >= 0.0)) {
-    const double dy0 = fmin(fmax(s.kx * X0, Y0), Y1), dy1 = fmin(fmax(s.kx * X1, Y0), Y1);
-    const double dx0 = fmin(fmax(s.ky * Y0, X0), X1), dx1 = fmin(fmax(s.ky * Y1, X0), X1);
-    const double e0 = (a * X0) * X0 + (b * X0) * dy0 + (c * dy0) * dy0;
-    const double e1 = (a * X1) * X1 + (b * X1) * dy1 + (c * dy1) * dy1;
-    const double e2 = (a * dx0) * dx0 + (b * dx0) * Y0 + (c * Y0) * Y0;
-    const double e3 = (a * dx1) * dx1 + (b * dx1) * Y1 + (c * Y1) * Y1;
-    emin = fmin(fmin(e0, e1), fmin(e2, e3));
-  }
-  const double ax = fmax(-X0, X1), ay = fmax(-Y0, Y1);
-  const double smax = (a * ax) * ax + (fabs(b) * ax) * ay + (c * ay) * ay;
-  const double thr = fmin((double)eCut, (double)s.eA + 1.0e-5) + 2.0e-6 * smax + 1.0e-6;
-  return emin <= thr;
+  float xl, xr;
+  if (!bandInterval(cq, ((float)(ty * tile) + 0.5f) - my, ((float)(ye - 1) + 0.5f) - my, xl, xr)) return false;
+  const float X0 = ((float)(tx * tile) + 0.5f) - mx;
+  const float X1 = ((float)(xe - 1) + 0.5f) - mx;
+  return X1 >= xl && X0 <= xr;
 }
 
 // sin(x) in double, |x| < 2^31: quadrant reduction by pi/2 (28-bit head so

@@ -47,7 +47,8 @@ struct ExpandArgs {
   const DevCam* cams;
   const uint32_t* sortedSlots;  // presorted (view, depth, id) order
   const uint2* rect;
-  const RenderRec* recs;        // read when cull != 0
+  const RenderRec* recs;        // read when cull != 0 (the mean)
+  const float4* cullRecs;       // read when cull != 0
   const uint8_t* dropped;
   const uint32_t* viewDrops;
   float eCut, aMin;

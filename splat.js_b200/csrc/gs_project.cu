@@ -114,31 +114,8 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
     const uint32_t y0 = u32sat(clampf(floorf((my - rad) / TF), 0.0f, (float)(ty - 1)));
     const uint32_t y1 = u32sat(clampf(floorf((my + rad) / TF), 0.0f, (float)(ty - 1)));
     a.rect[slot] = make_uint2(x0 | (y0 << 16), x1 | (y1 << 16));
-    // warp-block cull parameters, read when the rasteriser stages the entry.
-    // Completing the square in dx, a pixel (dx, dy) with exact exponent
-    // e <= t satisfies |dx - kA dy| <= sqrt(p - q dy^2), kA = -B / (2 hA),
-    // p = t / hA, q = (4 hA hC - B^2) / (4 hA^2).  t is the largest exponent
-    // the rasteriser can accept, min(eCut, ln(w / aMin)), plus margins for its
-    // FP32 evaluation (a few ulp of the largest term over the rectangle).  p
-    // is rounded up and q down, so the bound stays conservative; +inf = keep
-    // every warp (degenerate conic).
-    {
-      float4 cq = make_float4(__int_as_float(0x7F800000), 0.0f, 0.0f, 0.0f);
-      const double A = (double)r.r0.z, Bq = (double)r.r0.w, Cq = (double)r.r1.x;
-      const double det = 4.0 * A * Cq - Bq * Bq;
-      if (A > 0.0 && Cq > 0.0 && det > 0.0) {
-        const double dmx = (double)mx, dmy = (double)my, T = (double)a.tile;
-        const double ax = fmax(dmx - (double)x0 * T, (double)(x1 + 1) * T - dmx);
-        const double ay = fmax(dmy - (double)y0 * T, (double)(y1 + 1) * T - dmy);
-        const double smax = (A * ax) * ax + (fabs(Bq) * ax) * ay + (Cq * ay) * ay;
-        const double eA = (double)glog(r.r1.y / a.aMin);
-        const double tmax = fmin((double)a.eCut, eA + 1.0e-5) + 2.0e-6 * smax + 1.0e-6;
-        cq.x = __double2float_ru(tmax / A);
-        cq.y = __double2float_rd(det / (4.0 * A * A));
-        cq.z = __double2float_rn(-Bq / (2.0 * A));
-      }
-      a.cullRecs[slot] = cq;
-    }
+    // cull parameters: the tile cull and the rasteriser's warp-block masks
+    a.cullRecs[slot] = cullParams(mx, my, r.r0.z, r.r0.w, r.r1.x, r.r1.y, a.aMin, a.eCut, x0, x1, y0, y1, a.tile);
     // rectangle add on the (tx+1) x (ty+1) difference grid
     int32_t* gd = a.diffGrid + a.gridBase[v];
     const int gw = tx + 1;
@@ -315,7 +292,8 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
   uint32_t v = 0, i = 0, x0 = 0, y0 = 0, rw = 1, rc = 0, out = 0;
   bool test = false;
   unsigned long long mask = 0;
-  CullSplat cs{};
+  float mx = 0.0f, my = 0.0f;
+  float4 cq = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   s_run[threadIdx.x] = 0;
   if (!KEYS) s_mask[threadIdx.x] = 0;
   if (valid) {
@@ -330,8 +308,9 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
       rw = x1 - x0 + 1;
       test = a.cull && !(x0 == x1 && y0 == y1);
       if (test) {
-        const float4 q0 = a.recs[slot].r0, q1 = a.recs[slot].r1;
-        cs = cullPrep(q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, a.aMin);
+        const float4 q0 = a.recs[slot].r0;
+        mx = q0.x; my = q0.y;
+        cq = a.cullRecs[slot];
       }
       if (a.viewDrops[v] == 0) {
         rc = rw * (y1 - y0 + 1);
@@ -343,7 +322,7 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
           for (uint32_t x = x0; x <= x1; ++x) {
             const uint32_t t = y * c.tilesX + x;
             if (dr[t]) continue;
-            if (test && !tileLive(cs, a.eCut, (int)x, (int)y, a.tile, c.W, c.H)) continue;
+            if (test && !tileLive(cq, mx, my, (int)x, (int)y, a.tile, c.W, c.H)) continue;
             if (KEYS) {
               if (o < a.capacity) { a.keys[o] = c.tileBase + t; a.vals[o] = i; }
               else atomicOr(a.status, ST_ENTRY_OVERFLOW);
@@ -386,15 +365,13 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
     const uint32_t oout = __shfl_sync(FULL, out, lo);
     const bool otest = __shfl_sync(FULL, (uint32_t)test, lo) != 0u;
     const unsigned long long omask = KEYS ? __shfl_sync(FULL, mask, lo) : 0ull;
-    CullSplat ocs;
-    ocs.mx = __shfl_sync(FULL, cs.mx, lo);
-    ocs.my = __shfl_sync(FULL, cs.my, lo);
-    ocs.hA = __shfl_sync(FULL, cs.hA, lo);
-    ocs.B = __shfl_sync(FULL, cs.B, lo);
-    ocs.hC = __shfl_sync(FULL, cs.hC, lo);
-    ocs.eA = __shfl_sync(FULL, cs.eA, lo);
-    ocs.kx = __shfl_sync(FULL, cs.kx, lo);
-    ocs.ky = __shfl_sync(FULL, cs.ky, lo);
+    const float omx = __shfl_sync(FULL, mx, lo);
+    const float omy = __shfl_sync(FULL, my, lo);
+    float4 ocq;
+    ocq.x = __shfl_sync(FULL, cq.x, lo);
+    ocq.y = __shfl_sync(FULL, cq.y, lo);
+    ocq.z = __shfl_sync(FULL, cq.z, lo);
+    ocq.w = 0.0f;
     bool live = false;
     uint32_t gt = 0, k = 0;
     if (inRange) {
@@ -405,7 +382,7 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
       gt = c.tileBase + ty * (uint32_t)c.tilesX + tx;
       if (!otest) live = true;
       else if (KEYS && k < 64) live = ((omask >> k) & 1ull) != 0ull;
-      else live = tileLive(ocs, a.eCut, (int)tx, (int)ty, a.tile, c.W, c.H);
+      else live = tileLive(ocq, omx, omy, (int)tx, (int)ty, a.tile, c.W, c.H);
     }
     const uint32_t lb = __ballot_sync(FULL, live);
     const uint32_t peers = __match_any_sync(FULL, inRange ? (uint32_t)lo : 32u);

@@ -70,22 +70,12 @@ __device__ __forceinline__ uint32_t warp_block_mask(const float4 cq, float mx, f
   constexpr int NB = TILE / 4, WPR = TILE / 8;
   constexpr uint32_t ALL = NB * WPR >= 32 ? 0xFFFFFFFFu : (1u << (NB * WPR)) - 1u;
   if (!(cq.x < 3.0e38f)) return ALL;
-  const float p = cq.x, q = cq.y, kA = cq.z;
-  const float slackA = 4.0e-3f * (1.0f + fabsf(kA));
   uint32_t m = 0;
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
     const float Y0 = ((float)(ty * TILE + 4 * b) + 0.5f) - my;
-    const float Y1 = Y0 + 3.0f;
-    float d = Y0 > 0.0f ? Y0 : (Y1 < 0.0f ? -Y1 : 0.0f);
-    d = fmaxf(d - (1.0e-3f + 1.0e-6f * d), 0.0f);
-    const float rad2 = __fmaf_rn(-q, d * d, p) + 1.0e-5f * p;
-    if (!(rad2 >= 0.0f)) continue;
-    const float r = sqrtf(rad2) * 1.00001f;
-    const float c0 = kA * Y0, c1 = kA * Y1;
-    const float cl = fminf(c0, c1), ch = fmaxf(c0, c1);
-    const float sl = slackA + 1.0e-5f * (fabsf(cl) + fabsf(ch) + r);
-    const float xl = (cl - r) - sl, xr = (ch + r) + sl;
+    float xl, xr;
+    if (!bandInterval(cq, Y0, Y0 + 3.0f, xl, xr)) continue;
 #pragma unroll
     for (int wb = 0; wb < WPR; ++wb) {
       const float bx0 = ((float)(tx * TILE + 8 * wb) + 0.5f) - mx;

@@ -629,6 +629,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   ea.sortedSlots = sortedSlots;
   ea.rect = h->rect;
   ea.recs = h->recs;
+  ea.cullRecs = h->cullRecs;
   ea.dropped = h->dropped;
   ea.viewDrops = h->viewDrops;
   ea.eCut = h->o.eCut;
