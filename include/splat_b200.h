@@ -243,6 +243,13 @@ GS_API int gs_debug_binning(gs_trainer* h, uint32_t view, uint32_t* tileCnt, uin
 GS_API int gs_debug_pixels(gs_trainer* h, uint32_t view, float* rgba, float* finalT, uint32_t* endIdx);
 /* Fixed-point screen-space gradients of view slot `view`: n*10 i32
  * (shaders.js:26-28 slots 0-9); clear = 1 zeroes them afterwards. */
+/* Failure-detection check (no reference counterpart): runs one radix-sort
+ * pass whose decoupled look-back can never complete (its first block is
+ * never processed), so the waiting blocks give up after spinLimit spins
+ * (1 .. 2^22) and set the look-back-timeout bit (1) of the status word,
+ * returned in *statusOut with the kernel's time in ms.  Nothing hangs and the
+ * device stays usable; the trainer reports the same bit as GS_E_DEVICE. */
+GS_API int gs_debug_lookback_timeout(int32_t device, uint32_t spinLimit, uint32_t* statusOut, double* msOut);
 GS_API int gs_debug_gradp(gs_trainer* h, uint32_t view, int32_t* gradP10, int32_t clear);
 
 #ifdef __cplusplus

@@ -83,6 +83,7 @@ struct OnesweepArgs {
   uint32_t* statusWord;     // error bits
   const uint32_t* epoch;
   int pass;
+  uint32_t spinLimit;       // look-back spins before the block gives up and flags a timeout
 };
 
 struct RadixSortArgs {
@@ -187,6 +188,7 @@ uint32_t scan_partials_needed(uint64_t N);
 void launch_exclusive_scan(const uint32_t* in, uint64_t N, uint32_t* out, uint32_t* partials, uint32_t* total,
                            cudaStream_t s);
 int onesweep_grid(int device);
+int debug_lookback_timeout(int device, uint32_t spinLimit, uint32_t* statusOut, double* msOut);
 void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s);
 void launch_raster(const RasterArgs& a, int mode, bool stored, int tile, int batchDepth, unsigned grid,
                    cudaStream_t s);

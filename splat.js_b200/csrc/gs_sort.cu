@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_onesweep(OnesweepArgs a) {
           const uint32_t stag = (uint32_t)(s >> 32);
           const uint32_t flag = (uint32_t)(s >> 30) & 3u;
           if (stag != tag || flag == 0) {
-            if (++spins > LOOKBACK_SPIN_LIMIT) { atomicOr(a.statusWord, ST_LOOKBACK_TIMEOUT); break; }
+            if (++spins > a.spinLimit) { atomicOr(a.statusWord, ST_LOOKBACK_TIMEOUT); break; }
             __nanosleep(32);
             continue;
           }
@@ -397,6 +397,7 @@ static void radix_sort_t(const RadixSortArgs& a, cudaStream_t s) {
     o.statusWord = a.statusWord;
     o.epoch = a.epoch;
     o.pass = p;
+    o.spinLimit = LOOKBACK_SPIN_LIMIT;
     k_onesweep<KT><<<a.sweepGrid, RS_THREADS, rs_dyn_smem<KT>(), s>>>(o);
   }
 }
@@ -404,6 +405,64 @@ static void radix_sort_t(const RadixSortArgs& a, cudaStream_t s) {
 void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s) {
   if (a.keyBytes == 4) radix_sort_t<uint32_t>(a, s);
   else radix_sort_t<uint64_t>(a, s);
+}
+
+// ---------------------------------------------------------------------------
+// Failure-detection check: a look-back that can never complete.
+// One onesweep pass over 3 blocks of keys with the block counter starting at
+// 1, so block 0 is never processed and its status word is never published.
+// Blocks 1 and 2 wait on it, give up after `spinLimit` spins, flag
+// ST_LOOKBACK_TIMEOUT and finish (their scatter positions use a partial
+// prefix, which is smaller than the true one, so every store stays inside
+// the buffers).  Nothing hangs; the context stays usable.
+// ---------------------------------------------------------------------------
+int debug_lookback_timeout(int device, uint32_t spinLimit, uint32_t* statusOut, double* msOut) {
+  if (cudaSetDevice(device) != cudaSuccess) return -2;
+  const uint32_t n = 3u * RS_TILE;
+  uint32_t *keys = nullptr, *vals = nullptr, *outVals = nullptr, *small = nullptr;
+  uint64_t* status = nullptr;
+  int rc = 0;
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaMalloc(&keys, n * 4) != cudaSuccess || cudaMalloc(&vals, n * 4) != cudaSuccess ||
+      cudaMalloc(&outVals, n * 4) != cudaSuccess || cudaMalloc(&small, 4096 * 4) != cudaSuccess ||
+      cudaMalloc(&status, (size_t)8 * 256 * 8) != cudaSuccess || cudaStreamCreate(&s) != cudaSuccess ||
+      cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    rc = -3;
+  } else {
+    // small: [0, 2048) histograms, [2048, 2056) block counters, 2056 status word, 2057 epoch, 2058 count
+    cudaMemsetAsync(keys, 0, n * 4, s);
+    cudaMemsetAsync(vals, 0, n * 4, s);
+    cudaMemsetAsync(small, 0, 4096 * 4, s);
+    cudaMemsetAsync(status, 0, (size_t)8 * 256 * 8, s);
+    const uint32_t one = 1u;
+    cudaMemcpyAsync(small + 2048, &one, 4, cudaMemcpyHostToDevice, s);  // block 0 is never claimed
+    cudaMemcpyAsync(small + 2058, &n, 4, cudaMemcpyHostToDevice, s);
+    RadixHistArgs h;
+    h.keys = keys; h.nItems = small + 2058; h.hist = small; h.passes = 1; h.epoch = small + 2057;
+    k_radix_hist<uint32_t><<<4, 256, 0, s>>>(h);
+    OnesweepArgs o;
+    o.keysIn = keys; o.valsIn = vals; o.keysOut = nullptr; o.valsOut = outVals;
+    o.nItems = small + 2058; o.hist = small; o.tileCounter = small + 2048; o.status = status;
+    o.statusWord = small + 2056; o.epoch = small + 2057; o.pass = 0; o.spinLimit = spinLimit;
+    cudaFuncSetAttribute(k_onesweep<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)rs_dyn_smem<uint32_t>());
+    cudaEventRecord(e0, s);
+    k_onesweep<uint32_t><<<3, RS_THREADS, rs_dyn_smem<uint32_t>(), s>>>(o);
+    cudaEventRecord(e1, s);
+    uint32_t st = 0;
+    cudaMemcpyAsync(&st, small + 2056, 4, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = -2;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (statusOut) *statusOut = st;
+    if (msOut) *msOut = ms;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (s) cudaStreamDestroy(s);
+  cudaFree(keys); cudaFree(vals); cudaFree(outVals); cudaFree(small); cudaFree(status);
+  return rc;
 }
 
 }  // namespace gs

@@ -1156,6 +1156,12 @@ int gs_set_raster_config(gs_trainer* h, int32_t tile, int32_t batchDepth) {
   return GS_OK;
 }
 
+int gs_debug_lookback_timeout(int32_t device, uint32_t spinLimit, uint32_t* statusOut, double* msOut) {
+  if (spinLimit == 0 || spinLimit > (1u << 22)) return GS_E_INVALID;
+  const int rc = debug_lookback_timeout(device, spinLimit, statusOut, msOut);
+  return rc == 0 ? GS_OK : rc == -3 ? GS_E_NOMEM : GS_E_CUDA;
+}
+
 int gs_set_tile_cull(gs_trainer* h, int32_t enable) {
   if (!h) return GS_E_INVALID;
   if (enable != 0 && enable != 1) return fail(h, GS_E_INVALID, "tileCull must be 0 or 1");

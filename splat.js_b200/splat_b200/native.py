@@ -108,6 +108,7 @@ def lib():
         "gs_debug_records": (C.c_int, [H, C.c_uint32, f32p, u32p]),
         "gs_debug_binning": (C.c_int, [H, C.c_uint32, u32p, u32p, u32p, C.c_uint64, u64p]),
         "gs_debug_pixels": (C.c_int, [H, C.c_uint32, f32p, f32p, u32p]),
+        "gs_debug_lookback_timeout": (C.c_int, [C.c_int32, C.c_uint32, u32p, P(C.c_double)]),
         "gs_debug_gradp": (C.c_int, [H, C.c_uint32, i32p, C.c_int32]),
     }
     for name, (res, args) in sig.items():

@@ -69,3 +69,9 @@ def test_static_sort_rejects_sizes_above_its_limit():
     assert rc == N.GS_E_LIMIT
     hdr = open(os.path.join(ROOT, "include", "splat_b200.h")).read()
     assert "#define GS_STATIC_SORT_MAX (1u << 20)" in hdr
+
+
+def test_lookback_check_rejects_bad_spin_limits():
+    st, ms = C.c_uint32(), C.c_double()
+    assert N.lib().gs_debug_lookback_timeout(0, 0, C.byref(st), C.byref(ms)) == -1
+    assert N.lib().gs_debug_lookback_timeout(0, (1 << 22) + 1, C.byref(st), C.byref(ms)) == -1

@@ -433,3 +433,15 @@ def test_needles_and_discs_bitexact(tile):
     t, targets, metas = make(params, sh, [cam], [scene.uniform_target(256, 256, seed=21)], opts, radius=1.0)
     gpu_raster(t, [0], 3)
     check_view_against_oracle(t, oracle_opts(opts), oracle_cam(metas[0], 0, 1, 2), params, sh, targets, n)
+
+
+def test_lookback_timeout_is_reported_and_device_stays_usable():
+    """A sort pass whose look-back can never complete gives up after a bounded
+    number of spins, sets the timeout bit, and leaves the device usable."""
+    import ctypes as C
+    from splat_b200 import native as N
+    st, ms = C.c_uint32(), C.c_double()
+    N.check(N.lib().gs_debug_lookback_timeout(0, 1 << 16, C.byref(st), C.byref(ms)), None)
+    assert st.value & 1, st.value
+    assert ms.value < 5000.0, ms.value
+    test_gradcheck_rig_raster_bitexact()
