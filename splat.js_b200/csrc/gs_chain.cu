@@ -249,7 +249,12 @@ __global__ void __launch_bounds__(128, GS_CHAIN_MIN_BLOCKS) k_chain_view(ChainAr
   const int v = (int)(blockIdx.x - sb * (uint32_t)a.V);
   const uint32_t i = sb * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
-  const DevCam& c = a.cams[v];
+  // the block's camera in shared memory: read once, not re-fetched from
+  // global memory around every store
+  __shared__ DevCam s_cam;
+  if (threadIdx.x == 0) s_cam = a.cams[v];
+  __syncthreads();
+  const DevCam& c = s_cam;
   CamGrad7 cg = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f};
   if (i < a.n) {
     const size_t slot = (size_t)v * a.n + i;

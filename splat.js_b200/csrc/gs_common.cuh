@@ -23,6 +23,8 @@ constexpr int MAX_K = 15;           // SH rest coefficients per channel at degre
 
 // Device camera record: the Cam uniform of shaders.js:140-152 as
 // _camUniform fills it (trainer.js:357-372), plus derived tile geometry.
+constexpr int MAX_VIEWS = 16;  // most views one batched step can hold
+
 struct DevCam {
   float R[9];
   float t[3];

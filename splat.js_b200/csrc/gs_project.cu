@@ -32,6 +32,10 @@ template <int DEG>
 __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   constexpr int K = DEG > 0 ? (DEG + 1) * (DEG + 1) - 1 : 0;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  // the batch's cameras in shared memory (read once per block)
+  __shared__ DevCam s_cams[MAX_VIEWS];
+  for (int k = threadIdx.x; k < a.V; k += blockDim.x) s_cams[k] = a.cams[k];
+  __syncthreads();
   if (i >= a.n) return;
   float P[16];
   const float4* P4 = reinterpret_cast<const float4*>(a.params + (size_t)i * STRIDE);
@@ -45,7 +49,7 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   const float opa = sigm(P[13]);
 
   for (int v = 0; v < a.V; ++v) {
-    const DevCam& c = a.cams[v];
+    const DevCam& c = s_cams[v];
     const size_t slot = (size_t)v * a.n + i;
     a.rect[slot] = make_uint2(0xFFFFFFFFu, 0u);
     a.pkeys[slot] = ~0ull;

@@ -23,7 +23,7 @@ using namespace gs;
 
 namespace {
 
-constexpr int MAXB = 16;     // hard upper bound of views per batch
+constexpr int MAXB = MAX_VIEWS;  // hard upper bound of views per batch
 constexpr int RING = 8;      // pinned step-parameter slots
 
 struct StepParams {
