@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--batch-depth", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--profile-window", action="store_true",
+                    help="set up the workload, warm up, then run ONE batched step (tile 16, depth 256) between "
+                         "cudaProfilerStart/Stop for ncu --profile-from-start off; prints no bench line")
     return ap.parse_args()
 
 
@@ -290,6 +293,19 @@ def run_ours(args):
         images.append(dict(tw=c["w"], th=c["h"], rgb=np.ascontiguousarray(np.clip(img[..., :3], 0, 1).reshape(-1))))
     t.setup(dict(data=params, n=n, sh=sh), allcams, images, args.width, args.height, 4.0)
     del images
+    if args.profile_window:
+        t.iter = 2000
+        t.setRasterConfig(16, 256)
+        cs = list(range(B))
+        for _ in range(3):
+            t.stepBatch(cs)
+        N.check(N.lib().gs_sync(t._h), t._h)
+        torch.cuda.profiler.start()
+        t.stepBatch(cs)
+        N.check(N.lib().gs_sync(t._h), t._h)
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profile_window": "one batched step", "views": cs, "entries": t._state().lastEntries}))
+        return 0
     stream = torch.cuda.Stream(device=local)
     N.check(N.lib().gs_set_stream(t._h, C.c_void_p(stream.cuda_stream)), t._h)
     L = N.lib()
