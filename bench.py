@@ -38,6 +38,9 @@ for _p in (ROOT, os.path.join(ROOT, "splat.js_b200")):
 
 METRIC = "train views/s @1M splats 1080p, batched vs plain step, 1 B200, grads within 1e-4"
 FLOP_PER_PAIR = 26 + 70   # raster forward + backward per evaluated pixel-entry pair (FFMA = 2)
+# DRAM bytes (read + write) of one raster launch over an 8-view batch at the
+# default workload, from one ncu capture (not measured live)
+RASTER_DRAM_BYTES_8VIEW = 1.101793e9 + 0.461690e9
 
 
 def parse():
@@ -440,7 +443,11 @@ def run_ours(args):
                 "pairs_executed_per_step": pairs_exec,
                 "roofline": {"bound": "fp32", "kernel": "raster (fused forward + loss + backward)",
                              "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-                             "frac": achieved / peak.value if peak.value else None, "traffic": None,
+                             "frac": achieved / peak.value if peak.value else None,
+                             "traffic": RASTER_DRAM_BYTES_8VIEW if (B == 8 and n == 1_000_000 and args.width == 1920)
+                             else None,
+                             "traffic_source": "ncu capture of one 8-view step (cameras 0-7), "
+                                               "profiles/raster_16x256_step8_1M_1080p.md",
                              "peak_source": "gs_probe_fp32_peak FFMA kernel on this GPU (measured)",
                              "work": f"{FLOP_PER_PAIR} flop per pixel-entry pair P of the reference's tile lists "
                                      "(pairs up to each pixel's termination index); the step walks culled lists "
