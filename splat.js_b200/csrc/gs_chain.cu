@@ -21,7 +21,8 @@ struct CamGrad7 {
 };
 
 // chain for one visible splat in one view; gp = decoded screen-space grads
-// shp: the splat's SH coefficients (the caller stages them in shared memory).  The SH coefficient gradients are dRGB[c] * Y[k] for k < aK: the
+// shp: the splat's SH coefficients in global memory (read through the
+// cache).  The SH coefficient gradients are dRGB[c] * Y[k] for k < aK: the
 // gated dRGB, Y and aK are returned instead of the 3K products.
 template <int DEG>
 __device__ __forceinline__ void chainOne(const DevCam& c, const float* P, const Geom& g, float gp[10],
@@ -186,9 +187,9 @@ __device__ __forceinline__ void chainOne(const DevCam& c, const float* P, const 
 #pragma unroll
     for (int k = 0; k < K; ++k)
       if (k < aK) {
-        col[0] = col[0] + shp[k] * Yo[k];
-        col[1] = col[1] + shp[K + k] * Yo[k];
-        col[2] = col[2] + shp[2 * K + k] * Yo[k];
+        col[0] = col[0] + __ldg(shp + k) * Yo[k];
+        col[1] = col[1] + __ldg(shp + K + k) * Yo[k];
+        col[2] = col[2] + __ldg(shp + 2 * K + k) * Yo[k];
       }
 #pragma unroll
     for (int j = 0; j < 3; ++j) dRGB[j] = dRGB[j] * (col[j] > 0.0f ? 1.0f : 0.0f);
@@ -196,7 +197,7 @@ __device__ __forceinline__ void chainOne(const DevCam& c, const float* P, const 
 #pragma unroll
     for (int k = 0; k < K; ++k)
       if (k < aK) {
-        const float wk = dRGB[0] * shp[k] + dRGB[1] * shp[K + k] + dRGB[2] * shp[2 * K + k];
+        const float wk = dRGB[0] * __ldg(shp + k) + dRGB[1] * __ldg(shp + K + k) + dRGB[2] * __ldg(shp + 2 * K + k);
         float D[3];
         shBasisGradK<DEG>(k, vd, D);
 #pragma unroll
@@ -251,33 +252,7 @@ __global__ void __launch_bounds__(128, GS_CHAIN_MIN_BLOCKS) k_chain_view(ChainAr
   // the block's camera in shared memory: read once, not re-fetched from
   // global memory around every store
   __shared__ DevCam s_cam;
-  // the block's 128 splats' SH coefficients, copied with coalesced 16-byte
-  // loads, all issued before the first store (rows padded by one word, so
-  // each thread's row reads are conflict-free)
-  constexpr int SN = K > 0 ? 3 * K : 4;      // (the K = 0 instance never stages)
-  constexpr int SROW = K > 0 ? SN + 1 : 1;
-  __shared__ float s_sh[K > 0 ? 128 * SROW : 1];
   if (threadIdx.x == 0) s_cam = a.cams[v];
-  if (K > 0) {
-    const uint32_t i0 = sb * blockDim.x;
-    const uint32_t cnt = a.n - i0 < 128u ? a.n - i0 : 128u;
-    if ((SN & 3) == 0 && cnt == 128u) {
-      constexpr int Q = SN / 4;  // float4 per splat; 128 * Q float4 per block, Q per thread
-      const float4* g4 = reinterpret_cast<const float4*>(a.sh + (size_t)i0 * SN);
-      float4 q[Q];
-#pragma unroll
-      for (int u = 0; u < Q; ++u) q[u] = __ldg(g4 + threadIdx.x + 128 * u);
-#pragma unroll
-      for (int u = 0; u < Q; ++u) {
-        const uint32_t e = 4u * (threadIdx.x + 128u * (uint32_t)u);  // first float of this float4
-        float* d = s_sh + (e / SN) * SROW + e % SN;                   // SN % 4 == 0: stays in one row
-        d[0] = q[u].x; d[1] = q[u].y; d[2] = q[u].z; d[3] = q[u].w;
-      }
-    } else {
-      const float* gS = a.sh + (size_t)i0 * SN;
-      for (uint32_t e = threadIdx.x; e < cnt * SN; e += 128) s_sh[(e / SN) * SROW + e % SN] = __ldg(gS + e);
-    }
-  }
   __syncthreads();
   const DevCam& c = s_cam;
   CamGrad7 cg = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f};
@@ -313,7 +288,7 @@ __global__ void __launch_bounds__(128, GS_CHAIN_MIN_BLOCKS) k_chain_view(ChainAr
         const float lmax = cmid + sqrtf(fmaxf(cmid * cmid - (cva * cvc - g.vb * g.vb), 0.0f));
         const float cden = 1.0f + lmax;
         gp[2] = gp[2] * cden; gp[3] = gp[3] * cden; gp[4] = gp[4] * cden;
-        const float* shp = K > 0 ? s_sh + threadIdx.x * SROW : nullptr;
+        const float* shp = K > 0 ? a.sh + (size_t)i * 3 * K : nullptr;
         chainOne<DEG>(c, P, g, gp, shp, a.anisoReg, gF, dRGB, Y, vd, aK, cg);
       }
       float4* o = reinterpret_cast<float4*>(a.viewGrad + slot * VIEWGRAD_STRIDE);
