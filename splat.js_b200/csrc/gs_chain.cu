@@ -234,84 +234,78 @@ __device__ __forceinline__ void adamParam(const AdamHP& h, int slot, float& p, f
 #define GS_CHAIN_MIN_BLOCKS 5  // resident 128-thread blocks per SM the register allocation must allow
 #endif
 
-// Pass 1: one thread per (view, splat) item, taken in the presort's order:
-// the items that survived projection come first (in (view, depth) order) and
-// the culled ones last, so warps are either fully busy or exit at once.  A
-// visible splat's screen-space gradients are decoded (and cleared for the next
-// step) and chained through the view's camera; the result -- the 14 parameter
-// gradients, the gated colour gradient dRGB and the view direction (from
-// which the SH basis Y is recomputed) -- goes to viewGrad[slot] for pass 2.
-// Camera gradients are summed in fixed point (order-independent) over the
-// lanes of a warp that share a view, with one atomic per group.
+// Pass 1: one thread per (view, splat).  Blocks are ordered splat block major,
+// view minor, so the views of a splat block run together and its parameters
+// and SH coefficients are read from DRAM once.  A visible splat's screen-space
+// gradients are decoded (and cleared for the next step) and chained through
+// the view's camera; the result -- the 14 parameter gradients, the gated
+// colour gradient dRGB and the view direction (from which the SH basis Y is
+// recomputed) -- goes to viewGrad[slot] for pass 2.  Camera gradients are
+// summed per warp in fixed point (order-independent) with one atomic each.
 template <int DEG>
 __global__ void __launch_bounds__(128, GS_CHAIN_MIN_BLOCKS) k_chain_view(ChainArgs a) {
   constexpr int K = DEG > 0 ? (DEG + 1) * (DEG + 1) - 1 : 0;
-  const uint64_t items = (uint64_t)a.n * (uint64_t)a.V;
-  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t sb = blockIdx.x / (uint32_t)a.V;
+  const int v = (int)(blockIdx.x - sb * (uint32_t)a.V);
+  const uint32_t i = sb * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
-  // the batch's cameras in shared memory (read once per block)
-  __shared__ DevCam s_cams[MAX_VIEWS];
-  for (int k = threadIdx.x; k < a.V; k += blockDim.x) s_cams[k] = a.cams[k];
+  // the block's camera in shared memory: read once, not re-fetched from
+  // global memory around every store
+  __shared__ DevCam s_cam;
+  if (threadIdx.x == 0) s_cam = a.cams[v];
   __syncthreads();
-  uint32_t v = 0xFFFFFFFFu, i = 0;
-  size_t slot = 0;
-  if (p < items) {
-    slot = a.order[p];
-    v = (uint32_t)(slot / a.n);
-    i = (uint32_t)(slot - (size_t)v * a.n);
-  }
+  const DevCam& c = s_cam;
   CamGrad7 cg = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f};
-  if (p < items && a.rect[slot].x != 0xFFFFFFFFu) {
-    const DevCam& c = s_cams[v];
-    int4* G4 = reinterpret_cast<int4*>(a.gradP + slot * GP_STRIDE);
-    const int4 q0 = G4[0], q1 = G4[1], q2 = G4[2];
-    G4[0] = make_int4(0, 0, 0, 0);
-    G4[1] = make_int4(0, 0, 0, 0);
-    G4[2] = make_int4(0, 0, 0, 0);
-    const int32_t qi[10] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y};
-    float gp[10];
+  if (i < a.n) {
+    const size_t slot = (size_t)v * a.n + i;
+    if (a.rect[slot].x != 0xFFFFFFFFu) {
+      int4* G4 = reinterpret_cast<int4*>(a.gradP + slot * GP_STRIDE);
+      const int4 q0 = G4[0], q1 = G4[1], q2 = G4[2];
+      G4[0] = make_int4(0, 0, 0, 0);
+      G4[1] = make_int4(0, 0, 0, 0);
+      G4[2] = make_int4(0, 0, 0, 0);
+      const int32_t qi[10] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y};
+      float gp[10];
 #pragma unroll
-    for (int k = 0; k < 10; ++k) gp[k] = (float)qi[k] / ((k >= 2 && k <= 4) ? FIXEDC : FIXED);
-    float P[16];
-    const float4* P4 = reinterpret_cast<const float4*>(a.params + (size_t)i * STRIDE);
+      for (int k = 0; k < 10; ++k) gp[k] = (float)qi[k] / ((k >= 2 && k <= 4) ? FIXEDC : FIXED);
+      float P[16];
+      const float4* P4 = reinterpret_cast<const float4*>(a.params + (size_t)i * STRIDE);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const float4 t = __ldg(P4 + k);
-      P[4 * k] = t.x; P[4 * k + 1] = t.y; P[4 * k + 2] = t.z; P[4 * k + 3] = t.w;
+      for (int k = 0; k < 4; ++k) {
+        const float4 t = __ldg(P4 + k);
+        P[4 * k] = t.x; P[4 * k + 1] = t.y; P[4 * k + 2] = t.z; P[4 * k + 3] = t.w;
+      }
+      float gF[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) gF[k] = 0.0f;
+      float dRGB[3] = {0.0f, 0.0f, 0.0f}, vd[3] = {0.0f, 0.0f, 0.0f}, Y[15];
+      int aK = 0;
+      const Geom g = computeGeom(c, P);
+      if (g.ok) {
+        // undo the render pass's conic normalisation (shaders.js:735-744)
+        const float cva = g.va + 0.3f, cvc = g.vc + 0.3f;
+        const float cmid = 0.5f * (cva + cvc);
+        const float lmax = cmid + sqrtf(fmaxf(cmid * cmid - (cva * cvc - g.vb * g.vb), 0.0f));
+        const float cden = 1.0f + lmax;
+        gp[2] = gp[2] * cden; gp[3] = gp[3] * cden; gp[4] = gp[4] * cden;
+        const float* shp = K > 0 ? a.sh + (size_t)i * 3 * K : nullptr;
+        chainOne<DEG>(c, P, g, gp, shp, a.anisoReg, gF, dRGB, Y, vd, aK, cg);
+      }
+      float4* o = reinterpret_cast<float4*>(a.viewGrad + slot * VIEWGRAD_STRIDE);
+      o[0] = make_float4(gF[0], gF[1], gF[2], gF[3]);
+      o[1] = make_float4(gF[4], gF[5], gF[6], gF[7]);
+      o[2] = make_float4(gF[8], gF[9], gF[10], gF[11]);
+      o[3] = make_float4(gF[12], gF[13], dRGB[0], dRGB[1]);
+      o[4] = make_float4(dRGB[2], vd[0], vd[1], vd[2]);
     }
-    float gF[16];
-#pragma unroll
-    for (int k = 0; k < 16; ++k) gF[k] = 0.0f;
-    float dRGB[3] = {0.0f, 0.0f, 0.0f}, vd[3] = {0.0f, 0.0f, 0.0f}, Y[15];
-    int aK = 0;
-    const Geom g = computeGeom(c, P);
-    if (g.ok) {
-      // undo the render pass's conic normalisation (shaders.js:735-744)
-      const float cva = g.va + 0.3f, cvc = g.vc + 0.3f;
-      const float cmid = 0.5f * (cva + cvc);
-      const float lmax = cmid + sqrtf(fmaxf(cmid * cmid - (cva * cvc - g.vb * g.vb), 0.0f));
-      const float cden = 1.0f + lmax;
-      gp[2] = gp[2] * cden; gp[3] = gp[3] * cden; gp[4] = gp[4] * cden;
-      const float* shp = K > 0 ? a.sh + (size_t)i * 3 * K : nullptr;
-      chainOne<DEG>(c, P, g, gp, shp, a.anisoReg, gF, dRGB, Y, vd, aK, cg);
-    }
-    float4* o = reinterpret_cast<float4*>(a.viewGrad + slot * VIEWGRAD_STRIDE);
-    o[0] = make_float4(gF[0], gF[1], gF[2], gF[3]);
-    o[1] = make_float4(gF[4], gF[5], gF[6], gF[7]);
-    o[2] = make_float4(gF[8], gF[9], gF[10], gF[11]);
-    o[3] = make_float4(gF[12], gF[13], dRGB[0], dRGB[1]);
-    o[4] = make_float4(dRGB[2], vd[0], vd[1], vd[2]);
   }
-  // camera gradients: fixed-point sums over the warp's lanes of each view
-  const uint32_t peers = __match_any_sync(0xFFFFFFFFu, v);
-  if (v != 0xFFFFFFFFu && s_cams[v].train) {
-    const DevCam& c = s_cams[v];
+  // camera gradients: warp sums of the fixed-point values, one atomic each
+  if (c.train) {
     const float cv[7] = {cg.w[0], cg.w[1], cg.w[2], cg.t[0], cg.t[1], cg.t[2], cg.logf};
-    const int lead = __ffs(peers) - 1;
 #pragma unroll
     for (int k = 0; k < 7; ++k) {
-      const uint32_t r = __reduce_add_sync(peers, (uint32_t)fixq(cv[k], FIXCAM));
-      if (lane == lead && r) {
+      const uint32_t r = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)fixq(cv[k], FIXCAM));
+      if (lane == 0 && r) {
         const uint32_t idx = k < 6 ? c.camIdx * 8u + (uint32_t)k : c.ncams * 8u;
         atomicAdd(&a.gradCam[idx], (int32_t)r);
       }
@@ -441,7 +435,7 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
 void launch_chain_adam(const ChainArgs& a, int deg, cudaStream_t s) {
   const unsigned blocks = (a.n + 127) / 128;
   if (blocks == 0) return;
-  const unsigned g1 = (unsigned)(((uint64_t)a.n * (uint64_t)a.V + 127) / 128);
+  const unsigned g1 = blocks * (unsigned)a.V;
   switch (deg) {
     case 0: k_chain_view<0><<<g1, 128, 0, s>>>(a); k_chain_adam<0><<<blocks, 128, 0, s>>>(a); break;
     case 1: k_chain_view<1><<<g1, 128, 0, s>>>(a); k_chain_adam<1><<<blocks, 128, 0, s>>>(a); break;

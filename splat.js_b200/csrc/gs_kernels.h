@@ -141,7 +141,6 @@ struct ChainArgs {
   int32_t* gradP;
   const uint2* rect;
   float* viewGrad;         // V * n * VIEWGRAD_STRIDE: per-(view, splat) chain results
-  const uint32_t* order;   // V * n (view, splat) slots in presort order (visible items first)
   float anisoReg;
   int32_t* gradCam;
   float* gradF;            // optional readout (n * 16)

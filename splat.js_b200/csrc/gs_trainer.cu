@@ -720,7 +720,6 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
     c.gradP = h->gradP;
     c.rect = h->rect;
     c.viewGrad = h->viewGrad;
-    c.order = sortedSlots;
     c.anisoReg = h->o.anisoReg;
     c.gradCam = h->gradCam;
     c.gradF = sh.grads ? h->gradFOut : nullptr;
