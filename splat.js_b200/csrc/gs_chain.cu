@@ -234,9 +234,28 @@ __device__ __forceinline__ void adamParam(const AdamHP& h, int slot, float& p, f
 #define GS_CHAIN_MIN_BLOCKS 5  // resident 128-thread blocks per SM the register allocation must allow
 #endif
 
-// Pass 1: one thread per (view, splat).  Blocks are ordered splat block major,
-// view minor, so the views of a splat block run together and its parameters
-// and SH coefficients are read from DRAM once.  A visible splat's screen-space
+// Visible-item lists: for each view, the indices of the splats whose
+// rectangle survived projection, compacted with one atomic per warp.  The
+// order inside a list follows the warps' atomics (roughly ascending), which
+// pass 1 uses only for memory locality: each item's results go to its own
+// slot and camera gradients are integer sums, so no result depends on it.
+__global__ void __launch_bounds__(256) k_visible_list(ChainArgs a, uint32_t blocksPerView) {
+  const uint32_t v = blockIdx.x / blocksPerView;
+  const uint32_t i = (blockIdx.x - v * blocksPerView) * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool vis = i < a.n && a.rect[(size_t)v * a.n + i].x != 0xFFFFFFFFu;
+  const uint32_t b = __ballot_sync(0xFFFFFFFFu, vis);
+  if (!b) return;
+  uint32_t base = 0;
+  if (lane == 0) base = atomicAdd(&a.visCount[v], (uint32_t)__popc(b));
+  base = __shfl_sync(0xFFFFFFFFu, base, 0);
+  if (vis) a.visList[(size_t)v * a.n + base + (uint32_t)__popc(b & ((1u << lane) - 1u))] = i;
+}
+
+// Pass 1: one thread per visible (view, splat) item of the lists above.
+// Blocks are ordered list block major, view minor, so the views' items of
+// similar splat indices run together and their parameters and SH
+// coefficients are mostly read from DRAM once.  A visible splat's screen-space
 // gradients are decoded (and cleared for the next step) and chained through
 // the view's camera; the result -- the 14 parameter gradients, the gated
 // colour gradient dRGB and the view direction (from which the SH basis Y is
@@ -247,7 +266,11 @@ __global__ void __launch_bounds__(128, GS_CHAIN_MIN_BLOCKS) k_chain_view(ChainAr
   constexpr int K = DEG > 0 ? (DEG + 1) * (DEG + 1) - 1 : 0;
   const uint32_t sb = blockIdx.x / (uint32_t)a.V;
   const int v = (int)(blockIdx.x - sb * (uint32_t)a.V);
-  const uint32_t i = sb * blockDim.x + threadIdx.x;
+  const uint32_t pos = sb * blockDim.x + threadIdx.x;
+  const uint32_t cnt = a.visCount[v];
+  if (sb * blockDim.x >= cnt) return;  // the whole block is past the list (uniform)
+  const bool have = pos < cnt;
+  const uint32_t i = have ? a.visList[(size_t)v * a.n + pos] : 0u;
   const int lane = threadIdx.x & 31;
   // the block's camera in shared memory: read once, not re-fetched from
   // global memory around every store
@@ -256,9 +279,9 @@ __global__ void __launch_bounds__(128, GS_CHAIN_MIN_BLOCKS) k_chain_view(ChainAr
   __syncthreads();
   const DevCam& c = s_cam;
   CamGrad7 cg = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f};
-  if (i < a.n) {
+  if (have) {
     const size_t slot = (size_t)v * a.n + i;
-    if (a.rect[slot].x != 0xFFFFFFFFu) {
+    {
       int4* G4 = reinterpret_cast<int4*>(a.gradP + slot * GP_STRIDE);
       const int4 q0 = G4[0], q1 = G4[1], q2 = G4[2];
       G4[0] = make_int4(0, 0, 0, 0);
@@ -436,6 +459,8 @@ void launch_chain_adam(const ChainArgs& a, int deg, cudaStream_t s) {
   const unsigned blocks = (a.n + 127) / 128;
   if (blocks == 0) return;
   const unsigned g1 = blocks * (unsigned)a.V;
+  const unsigned bpv = (a.n + 255) / 256;
+  k_visible_list<<<bpv * (unsigned)a.V, 256, 0, s>>>(a, bpv);
   switch (deg) {
     case 0: k_chain_view<0><<<g1, 128, 0, s>>>(a); k_chain_adam<0><<<blocks, 128, 0, s>>>(a); break;
     case 1: k_chain_view<1><<<g1, 128, 0, s>>>(a); k_chain_adam<1><<<blocks, 128, 0, s>>>(a); break;

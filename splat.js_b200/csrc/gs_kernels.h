@@ -141,6 +141,8 @@ struct ChainArgs {
   int32_t* gradP;
   const uint2* rect;
   float* viewGrad;         // V * n * VIEWGRAD_STRIDE: per-(view, splat) chain results
+  uint32_t* visList;       // V * n: per view, indices of the visible splats
+  uint32_t* visCount;      // V counters, cleared before the step
   float anisoReg;
   int32_t* gradCam;
   float* gradF;            // optional readout (n * 16)
