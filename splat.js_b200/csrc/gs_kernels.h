@@ -55,7 +55,6 @@ struct ExpandArgs {
   int tile;
   int cull;                     // 1: keep only entries tileLive() accepts
   uint32_t* counts;             // count pass: V * n, in presorted order
-  unsigned long long* liveMask; // V * n: tile-test results of each item's first 64 candidates
   const uint32_t* offsets;      // key pass: V * n exclusive scan of counts
   uint32_t* keys;               // global tile id per entry
   uint32_t* vals;               // splat id per entry

@@ -268,48 +268,76 @@ __global__ void k_tile_ranges_finish(TileRangeArgs a, uint32_t totalTiles) {
   a.ranges[gt] = make_uint2(r.x + base, r.y + base);
 }
 
+// The live columns of one tile row of an item's rectangle.  tileLive(tx, ty)
+// is X1(tx) >= xl && X0(tx) <= xr for the row's band interval [xl, xr], with
+// X0 and X1 non-decreasing in tx, so the live tiles of a row form one run
+// [ca, cb]; two binary searches on the same predicates find it, giving
+// exactly the tiles tileLive() accepts.  Returns the run length (0: none).
+__device__ __forceinline__ uint32_t row_run(const float4 cq, float mx, float my, uint32_t x0, uint32_t x1,
+                                            uint32_t ty, int tile, int W, int H, uint32_t& ca) {
+  ca = x0;
+  if (!(cq.x < 3.0e38f)) return x1 - x0 + 1;
+  const int ye = (int)ty * tile + tile < H ? (int)ty * tile + tile : H;
+  float xl, xr;
+  if (!bandInterval(cq, ((float)((int)ty * tile) + 0.5f) - my, ((float)(ye - 1) + 0.5f) - my, xl, xr)) return 0;
+  // ca: first column with X1 >= xl
+  uint32_t lo = x0, hi = x1 + 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    const int xe = (int)mid * tile + tile < W ? (int)mid * tile + tile : W;
+    if (((float)(xe - 1) + 0.5f) - mx >= xl) hi = mid;
+    else lo = mid + 1;
+  }
+  ca = lo;
+  // cb + 1: first column after ca with X0 > xr
+  hi = x1 + 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (((float)((int)mid * tile) + 0.5f) - mx <= xr) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo - ca;
+}
+
 // Entry expansion of the presorted items, in two passes over the same walk:
 // KEYS = false counts each item's entries, KEYS = true writes them at the
 // counts' exclusive scan -- key = global tile id, value = splat id, tiles of
 // an item in row order.  An entry is a tile of the item's rectangle that the
 // entry budget kept and, with culling on, that tileLive() accepts (a
-// single-tile rectangle is kept untested).  The count pass records the test's
-// results for an item's first 64 candidates in liveMask, which the key pass
-// reads instead of testing again.
+// single-tile rectangle is kept untested).
 //
-// A warp walks the candidate (item, tile) pairs of its 32 items 32 at a time:
-// each lane finds the item owning its candidate by a binary search over the
-// items' candidate offsets (shuffles), tests the tile, and a ballot ranks the
-// accepted candidates of each item; so stores are coalesced and no lane waits
-// on a large splat.  Items of views that dropped tiles to the budget are
-// walked by their own lane (rare).
+// A warp walks the tile rows of its 32 items 32 rows at a time: each lane
+// finds the item owning its row by a binary search over the items' row
+// offsets (shuffles) and computes the row's run of live tiles.  The count
+// pass sums the runs per item; the key pass ranks them (a segmented scan) and
+// then fills the rows' outputs 32 entries at a time, each lane finding its
+// row by a second binary search, so stores are coalesced.  Items of views
+// that dropped tiles to the budget are walked by their own lane (rare).
 template <bool KEYS>
 __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
-  __shared__ uint32_t s_run[256];                 // entries of each item so far
-  __shared__ unsigned long long s_mask[KEYS ? 1 : 256];  // count pass: test results
+  __shared__ uint32_t s_run[256];  // entries of each item so far
   const uint64_t items = (uint64_t)a.n * a.V;
   const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const int wbase = threadIdx.x & ~31;
   const uint32_t FULL = 0xFFFFFFFFu;
+  const uint32_t ltm = (1u << lane) - 1u;
   const bool valid = p < items;
-  uint32_t v = 0, i = 0, x0 = 0, y0 = 0, rw = 1, rc = 0, out = 0;
+  uint32_t v = 0, i = 0, x0 = 0, x1 = 0, y0 = 0, rr = 0, out = 0;
   bool test = false;
-  unsigned long long mask = 0;
   float mx = 0.0f, my = 0.0f;
-  float4 cq = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  float4 cq = make_float4(__int_as_float(0x7F800000), 0.0f, 0.0f, 0.0f);
   s_run[threadIdx.x] = 0;
-  if (!KEYS) s_mask[threadIdx.x] = 0;
   if (valid) {
     const uint32_t slot = a.sortedSlots[p];
     const uint2 r = a.rect[slot];
-    if (KEYS) { out = a.offsets[p]; if (a.cull) mask = a.liveMask[p]; }
+    if (KEYS) out = a.offsets[p];
     if (r.x != 0xFFFFFFFFu) {
       v = slot / a.n;
       i = slot - v * a.n;
       x0 = r.x & 0xFFFFu; y0 = r.x >> 16;
-      const uint32_t x1 = r.y & 0xFFFFu, y1 = r.y >> 16;
-      rw = x1 - x0 + 1;
+      x1 = r.y & 0xFFFFu;
+      const uint32_t y1 = r.y >> 16;
       test = a.cull && !(x0 == x1 && y0 == y1);
       if (test) {
         const float4 q0 = a.recs[slot].r0;
@@ -317,7 +345,7 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
         cq = a.cullRecs[slot];
       }
       if (a.viewDrops[v] == 0) {
-        rc = rw * (y1 - y0 + 1);
+        rr = y1 - y0 + 1;
       } else {
         const DevCam& c = a.cams[v];
         const uint8_t* dr = a.dropped + c.tileBase;
@@ -338,37 +366,32 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
       }
     }
   }
+  if (!test) cq = make_float4(__int_as_float(0x7F800000), 0.0f, 0.0f, 0.0f);  // untested: whole rows
   __syncwarp();
-  // candidate offsets of the warp's items (inclusive scan of rc)
-  uint32_t cEnd = rc;
+  // row offsets of the warp's items (inclusive scan of rr)
+  uint32_t rEnd = rr;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(FULL, cEnd, o);
-    if (lane >= o) cEnd += y;
+    const uint32_t y = __shfl_up_sync(FULL, rEnd, o);
+    if (lane >= o) rEnd += y;
   }
-  const uint32_t cBase = cEnd - rc;
-  const uint32_t C = __shfl_sync(FULL, cEnd, 31);
-  const uint32_t ltm = (1u << lane) - 1u;
-  for (uint32_t base = 0; base < C; base += 32) {
-    const uint32_t e = base + (uint32_t)lane;
-    const bool inRange = e < C;
-    // owner: the last lane whose candidate offset is <= e; lanes without
-    // candidates share their successor's offset, so the last one holds e
+  const uint32_t rBase = rEnd - rr;
+  const uint32_t R = __shfl_sync(FULL, rEnd, 31);
+  for (uint32_t base = 0; base < R; base += 32) {
+    const uint32_t u = base + (uint32_t)lane;
+    const bool inRange = u < R;
+    // owner: the last lane whose row offset is <= u
     int lo = 0;
 #pragma unroll
     for (int step = 16; step >= 1; step >>= 1) {
-      const uint32_t ob = __shfl_sync(FULL, cBase, (lo + step) & 31);
-      if (lo + step < 32 && ob <= e) lo += step;
+      const uint32_t ob = __shfl_sync(FULL, rBase, (lo + step) & 31);
+      if (lo + step < 32 && ob <= u) lo += step;
     }
-    const uint32_t ocb = __shfl_sync(FULL, cBase, lo);
-    const uint32_t ox = __shfl_sync(FULL, x0, lo);
-    const uint32_t oy = __shfl_sync(FULL, y0, lo);
-    const uint32_t orw = __shfl_sync(FULL, rw, lo);
+    const uint32_t orb = __shfl_sync(FULL, rBase, lo);
+    const uint32_t ox0 = __shfl_sync(FULL, x0, lo);
+    const uint32_t ox1 = __shfl_sync(FULL, x1, lo);
+    const uint32_t oy0 = __shfl_sync(FULL, y0, lo);
     const uint32_t ov = __shfl_sync(FULL, v, lo);
-    const uint32_t oi = __shfl_sync(FULL, i, lo);
-    const uint32_t oout = __shfl_sync(FULL, out, lo);
-    const bool otest = __shfl_sync(FULL, (uint32_t)test, lo) != 0u;
-    const unsigned long long omask = KEYS ? __shfl_sync(FULL, mask, lo) : 0ull;
     const float omx = __shfl_sync(FULL, mx, lo);
     const float omy = __shfl_sync(FULL, my, lo);
     float4 ocq;
@@ -376,39 +399,69 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
     ocq.y = __shfl_sync(FULL, cq.y, lo);
     ocq.z = __shfl_sync(FULL, cq.z, lo);
     ocq.w = 0.0f;
-    bool live = false;
-    uint32_t gt = 0, k = 0;
+    uint32_t cnt = 0, ca = 0, ty = 0;
     if (inRange) {
-      k = e - ocb;
-      const uint32_t ry = k / orw, rx = k - ry * orw;
-      const uint32_t tx = ox + rx, ty = oy + ry;
+      ty = oy0 + (u - orb);
       const DevCam& c = a.cams[ov];
-      gt = c.tileBase + ty * (uint32_t)c.tilesX + tx;
-      if (!otest) live = true;
-      else if (KEYS && k < 64) live = ((omask >> k) & 1ull) != 0ull;
-      else live = tileLive(ocq, omx, omy, (int)tx, (int)ty, a.tile, c.W, c.H);
+      cnt = row_run(ocq, omx, omy, ox0, ox1, ty, a.tile, c.W, c.H, ca);
     }
-    const uint32_t lb = __ballot_sync(FULL, live);
     const uint32_t peers = __match_any_sync(FULL, inRange ? (uint32_t)lo : 32u);
-    const uint32_t prior = s_run[wbase + lo];
-    if (KEYS && live) {
-      const uint32_t o = oout + prior + __popc(lb & peers & ltm);
-      if (o < a.capacity) { a.keys[o] = gt; a.vals[o] = oi; }
-      else atomicOr(a.status, ST_ENTRY_OVERFLOW);
-    }
-    __syncwarp();
     const int lead = __ffs(peers) - 1;
-    if (inRange && lane == lead) {
-      s_run[wbase + lo] = prior + __popc(lb & peers);
-      // the group's candidates are consecutive: bit j of (lb & peers) >> lead is candidate k + j
-      if (!KEYS && k < 64) s_mask[wbase + lo] |= (unsigned long long)((lb & peers) >> lead) << k;
+    const uint32_t prior = s_run[wbase + lo];
+    // segmented scan of the run lengths over the rows of each item
+    uint32_t inc = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, inc, o);
+      if (lane >= o) inc += y;
     }
+    const uint32_t before = __shfl_sync(FULL, inc, lead > 0 ? lead - 1 : 0);
+    const uint32_t segIncl = inc - (lead > 0 ? before : 0u);  // rows of this item up to this lane
+    if (KEYS) {
+      // this row's entries start here; fill the chunk's outputs 32 at a time
+      const uint32_t oout = __shfl_sync(FULL, out, lo);
+      const uint32_t rowOut = oout + prior + segIncl - cnt;
+      const uint32_t oi = __shfl_sync(FULL, i, lo);
+      const uint32_t tileBase = a.cams[ov].tileBase, tilesX = (uint32_t)a.cams[ov].tilesX;
+      const uint32_t rowKey = tileBase + ty * tilesX + ca;  // key of the run's first tile
+      // the chunk's rows in output order: rowOut is non-decreasing over lanes with entries
+      const uint32_t firstOut = __reduce_min_sync(FULL, cnt ? rowOut : 0xFFFFFFFFu);
+      uint32_t lastEnd = __reduce_max_sync(FULL, cnt ? rowOut + cnt : 0u);
+      // 32 rows hold at most 32 x 65535 tiles; anything larger is corrupt input
+      if (lastEnd > firstOut && lastEnd - firstOut > 32u * 65535u) {
+        if (lane == 0) atomicOr(a.status, ST_BAD_INPUT);
+        lastEnd = firstOut;
+      }
+      for (uint32_t eb = firstOut; eb < lastEnd; eb += 32) {
+        const uint32_t e = eb + (uint32_t)lane;
+        // the last lane with entries whose rowOut <= e
+        int w = -1;
+        // non-decreasing over lanes: rows without entries keep their start
+        const uint32_t key = inRange ? rowOut : 0xFFFFFFFFu;
+        int l2 = 0;
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+          const uint32_t kb = __shfl_sync(FULL, key, (l2 + step) & 31);
+          if (l2 + step < 32 && kb <= e) l2 += step;
+        }
+        const uint32_t k0 = __shfl_sync(FULL, key, l2);
+        w = (k0 <= e) ? l2 : -1;
+        const uint32_t wc = __shfl_sync(FULL, cnt, l2 & 31);
+        const uint32_t wk = __shfl_sync(FULL, rowKey, l2 & 31);
+        const uint32_t wi = __shfl_sync(FULL, oi, l2 & 31);
+        if (w >= 0 && e < lastEnd && e - k0 < wc) {
+          if (e < a.capacity) { a.keys[e] = wk + (e - k0); a.vals[e] = wi; }
+          else atomicOr(a.status, ST_ENTRY_OVERFLOW);
+        }
+      }
+    }
+    uint32_t gsum = 0;
+    if (inRange) gsum = __reduce_add_sync(peers, cnt);  // the lanes of one item call it together
+    __syncwarp();
+    if (inRange && lane == lead) s_run[wbase + lo] = prior + gsum;
     __syncwarp();
   }
-  if (!KEYS && valid) {
-    a.counts[p] = s_run[threadIdx.x];
-    if (a.cull) a.liveMask[p] = s_mask[threadIdx.x];
-  }
+  if (!KEYS && valid) a.counts[p] = s_run[threadIdx.x];
 }
 
 // Per-tile ranges from the sorted entry keys (culled lists): tile gt spans

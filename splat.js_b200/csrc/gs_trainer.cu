@@ -78,7 +78,6 @@ struct gs_trainer {
   RenderRec* recs = nullptr;
   uint2* rect = nullptr;
   uint32_t *counts = nullptr, *offsets = nullptr;
-  unsigned long long* liveMask = nullptr;
   float4* cullRecs = nullptr;
   float* viewGrad = nullptr;
   uint32_t* visList = nullptr;
@@ -384,7 +383,6 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   GS_AL(h->rect, (size_t)B * cap);
   GS_AL(h->counts, (size_t)B * cap);
   GS_AL(h->offsets, (size_t)B * cap);
-  GS_AL(h->liveMask, (size_t)B * cap);
   GS_AL(h->cullRecs, (size_t)B * cap);
   GS_AL(h->viewGrad, (size_t)B * cap * VIEWGRAD_STRIDE);
   GS_AL(h->visList, (size_t)B * cap);
@@ -640,7 +638,6 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   ea.tile = sh.tile;
   ea.cull = cull ? 1 : 0;
   ea.counts = h->counts;
-  ea.liveMask = h->liveMask;
   ea.offsets = h->offsets;
   ea.keys = h->keys[0];
   ea.vals = h->vals[0];
@@ -883,6 +880,7 @@ static int check_status(gs_trainer* h) {
     std::string m = "device status:";
     if (st & ST_LOOKBACK_TIMEOUT) m += " sort look-back wait exceeded its limit;";
     if (st & ST_ENTRY_OVERFLOW) m += " entry buffer overflow;";
+    if (st & ST_BAD_INPUT) m += " inconsistent entry expansion;";
     return fail(h, GS_E_DEVICE, m);
   }
   return GS_OK;
