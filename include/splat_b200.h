@@ -232,7 +232,7 @@ GS_API int gs_set_tile_cull(gs_trainer* h, int32_t enable);
  * ci[0..nviews); mode 1 = forward only, 3 = forward + loss + backward. */
 GS_API int gs_raster_pass(gs_trainer* h, const uint32_t* ci, uint32_t nviews, int32_t mode);
 /* Per-splat raster record of view slot `view`: rec n*12 f32
- * (mx, my, cA/2, cB, cC/2, opa*comp, r, g, b, opa, 1/(1+lambda_max), cull radius),
+ * (mx, my, cA/2, cB, cC/2, opa*comp, r, g, b, opa, -1/(2(1+lambda_max)), 1 - opa),
  * rect n*2 u32 (x0 | y0<<16, x1 | y1<<16; 0xFFFFFFFF = culled). */
 GS_API int gs_debug_records(gs_trainer* h, uint32_t view, float* rec12, uint32_t* rect2);
 /* Binning of view slot `view`: tileCnt[tiles], ranges[2*tiles] (global entry

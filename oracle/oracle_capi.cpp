@@ -91,7 +91,8 @@ void oracle_project_f64(const OOpts* oo, const OCam* oc, const double* params, c
 }
 
 // Per-splat values the rasteriser reads, derived from proj exactly as the
-// render pass does (w = opa*comp, cnorm = 1/(1+lambda_max), cull radius), plus tile
+// render pass does (w = opa*comp, -cnorm/2 with cnorm = 1/(1+lambda_max),
+// 1 - opa), in the CUDA library's record layout, plus tile
 // bounds packed {x0 | y0<<16, x1 | y1<<16} ({~0, 0} when culled).
 void oracle_records_f32(const OOpts* oo, const OCam* oc, const float* proj, uint32_t n, float* rec12,
                         uint32_t* rect2) {
@@ -106,10 +107,8 @@ void oracle_records_f32(const OOpts* oo, const OCam* oc, const float* proj, uint
       continue;
     }
     const Splat2D<float> s = splat2D<float>(pr);
-    // the rasteriser's conservative whole-warp cull radius: rad + 1 px, or
-    // unbounded when the radius clamp (radClamp * W) was active
-    const float cullR = pr[15] >= o.radClamp * (float)c.W ? INFINITY : pr[15] + 1.0f;
-    const float v[12] = {s.mx, s.my, 0.5f * s.cA, s.cB, 0.5f * s.cC, s.w, s.r, s.g, s.b, s.opa, s.cnorm, cullR};
+    const float v[12] = {s.mx, s.my, 0.5f * s.cA, s.cB, 0.5f * s.cC, s.w, s.r, s.g, s.b, s.opa, -0.5f * s.cnorm,
+                         1.0f - s.opa};
     for (int k = 0; k < 12; ++k) r[k] = v[k];
     const TileRect t = tileRect<float>(c, o.tile, pr[0], pr[1], pr[15]);
     rect2[2 * i] = (uint32_t)t.x0 | ((uint32_t)t.y0 << 16);

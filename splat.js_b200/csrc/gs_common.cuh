@@ -44,7 +44,7 @@ struct DevCam {
 };
 
 // Per-(view, splat) record read by the rasteriser: 3 x float4 = 48 B.
-//   r0 = (mx, my, cA/2, cB)  r1 = (cC/2, w = opa*comp, r, g)  r2 = (b, opa, cnorm, cull radius)
+//   r0 = (mx, my, cA/2, cB)  r1 = (cC/2, w = opa*comp, r, g)  r2 = (b, opa, -cnorm/2, 1 - opa)
 struct __align__(16) RenderRec {
   float4 r0, r1, r2;
 };

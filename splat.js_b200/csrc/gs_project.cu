@@ -97,16 +97,14 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
     // as 1/(1 + (mid + disc)) computed here from identical operands
     const float lmax = mid + disc;
     const float cnorm = 1.0f / (1.0f + lmax);
-    // conservative cull radius for whole warps of pixels: beyond `rad` from the
-    // mean no pixel passes both cutoffs (e >= d^2 / (2 lambda_max) > eMax),
-    // unless the radius was clamped; one pixel of margin covers rounding
-    const float cullR = rad >= a.radClamp * (float)c.W ? __int_as_float(0x7F800000) : rad + 1.0f;
+    // the backward reads -cnorm/2 and 1 - opa (exact or identically rounded
+    // forms of its own factors), stored here once per (view, splat)
     RenderRec r;
     // conic stored as (cA/2, cB, cC/2): halving is exact and saves the
     // rasteriser's per-pixel multiplies by 0.5
     r.r0 = make_float4(mx, my, 0.5f * (cd * inv), -g.vb * inv);
     r.r1 = make_float4(0.5f * (ad * inv), opa * comp, col[0], col[1]);
-    r.r2 = make_float4(col[2], opa, cnorm, cullR);
+    r.r2 = make_float4(col[2], opa, -0.5f * cnorm, 1.0f - opa);
     a.recs[slot] = r;
     a.pkeys[slot] = ((unsigned long long)v << 32) | __float_as_uint(g.pc[2]);
 

@@ -51,12 +51,6 @@ __device__ __forceinline__ float pairExponent(const float4& r0, float hC, float 
 // trunc(clamp(x, -1e9, 1e9)) for an already scaled value
 __device__ __forceinline__ int32_t fix_scaled(float x) { return __float2int_rz(fminf(fmaxf(x, -1.0e9f), 1.0e9f)); }
 
-// warp-uniform: can the splat reach any pixel centre of the warp's 8x4 block?
-__device__ __forceinline__ bool warpTouches(const float4& r0, float cullR, float wcx, float wcy) {
-  const float ox = fmaxf(fabsf(r0.x - wcx) - 3.5f, 0.0f);
-  const float oy = fmaxf(fabsf(r0.y - wcy) - 1.5f, 0.0f);
-  return ox * ox + oy * oy <= cullR * cullR;
-}
 
 // Which of the tile's 8x4 warp blocks can the splat reach?  Bit w = warp w
 // (block row w / (TILE/8), column w % (TILE/8)).  For each 4-row band, the
@@ -105,6 +99,7 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
   __shared__ uint32_t s_item;
   __shared__ uint32_t s_redu[NW][5];
   __shared__ uint32_t s_endmax[NW];
+  __shared__ __align__(16) int32_t s_stage[BWD ? NW : 1][12];  // per warp: the 10 sums of one entry
 
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int lx = (wid % WPR) * 8 + (lane & 7);
@@ -321,7 +316,6 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
             const float4 r0 = rr.r0;
             const float4 r1 = rr.r1;
             const float4 r2 = rr.r2;
-            if (!haveBits && !warpTouches(r0, r2.w, wcx, wcy)) continue;
             // Straight-line body, predicated per lane: lanes that do not
             // composite this entry (past their end, outside a cutoff) compute
             // on a clamped exponent and have their contribution zeroed
@@ -345,7 +339,7 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
             const float gal16 = c2 ? galpha * FIXED : 0.0f;
             const float ga16 = gal16 * araw;
             const float cA = r0.z + r0.z, cC = r1.x + r1.x;  // exact doubling of the stored halves
-            const float gq16 = ga16 * (-0.5f * r2.z);
+            const float gq16 = ga16 * r2.z;  // r2.z = -cnorm / 2
             const float gqx16 = gq16 * dx;
             float xs[10];
             xs[0] = ga16 * __fmaf_rn(cA, dx, r0.w * dy);
@@ -354,7 +348,7 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
             xs[3] = (gqx16 * dy) * 2.0f;
             xs[4] = (gq16 * dy) * dy;
             xs[5] = (gal16 * r2.y) * G;
-            xs[6] = ga16 * (1.0f - r2.y);
+            xs[6] = ga16 * r2.w;  // r2.w = 1 - opacity
             xs[7] = g16_0 * aT;
             xs[8] = g16_1 * aT;
             xs[9] = g16_2 * aT;
@@ -372,11 +366,16 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
               S2 = __fmaf_rn(r2.x, aT, S2);
               Ta = Tb;
             }
+            // lane 0 stages the 10 warp sums; lanes 0-9 add one each
             if (lane == 0) {
-              int32_t* acc = s_acc + (j - lo) * 10;
-#pragma unroll
-              for (int k = 0; k < 10; ++k) atomicAdd(&acc[k], (int32_t)rsum[k]);
+              int4* st = reinterpret_cast<int4*>(s_stage[wid]);
+              st[0] = make_int4((int)rsum[0], (int)rsum[1], (int)rsum[2], (int)rsum[3]);
+              st[1] = make_int4((int)rsum[4], (int)rsum[5], (int)rsum[6], (int)rsum[7]);
+              reinterpret_cast<int2*>(s_stage[wid])[4] = make_int2((int)rsum[8], (int)rsum[9]);
             }
+            __syncwarp();
+            if (lane < 10) atomicAdd(&s_acc[(j - lo) * 10 + (uint32_t)lane], s_stage[wid][lane]);
+            __syncwarp();
           }
         }
         __syncthreads();
