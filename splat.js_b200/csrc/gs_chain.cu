@@ -235,21 +235,27 @@ __device__ __forceinline__ void adamParam(const AdamHP& h, int slot, float& p, f
 #endif
 
 // Visible-item lists: for each view, the indices of the splats whose
-// rectangle survived projection, compacted with one atomic per warp.  The
-// order inside a list follows the warps' atomics (roughly ascending), which
+// rectangle survived projection, compacted with one atomic per block.  The
+// order inside a list follows the blocks' atomics (roughly ascending), which
 // pass 1 uses only for memory locality: each item's results go to its own
 // slot and camera gradients are integer sums, so no result depends on it.
 __global__ void __launch_bounds__(256) k_visible_list(ChainArgs a, uint32_t blocksPerView) {
+  __shared__ uint32_t s_warp[8];
+  __shared__ uint32_t s_base;
   const uint32_t v = blockIdx.x / blocksPerView;
   const uint32_t i = (blockIdx.x - v * blocksPerView) * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const bool vis = i < a.n && a.rect[(size_t)v * a.n + i].x != 0xFFFFFFFFu;
   const uint32_t b = __ballot_sync(0xFFFFFFFFu, vis);
-  if (!b) return;
-  uint32_t base = 0;
-  if (lane == 0) base = atomicAdd(&a.visCount[v], (uint32_t)__popc(b));
-  base = __shfl_sync(0xFFFFFFFFu, base, 0);
-  if (vis) a.visList[(size_t)v * a.n + base + (uint32_t)__popc(b & ((1u << lane) - 1u))] = i;
+  if (lane == 0) s_warp[wid] = (uint32_t)__popc(b);
+  __syncthreads();
+  if (threadIdx.x == 0) {  // one atomic per block
+    uint32_t t = 0;
+    for (int w = 0; w < 8; ++w) { const uint32_t c = s_warp[w]; s_warp[w] = t; t += c; }
+    s_base = t ? atomicAdd(&a.visCount[v], t) : 0u;
+  }
+  __syncthreads();
+  if (vis) a.visList[(size_t)v * a.n + s_base + s_warp[wid] + (uint32_t)__popc(b & ((1u << lane) - 1u))] = i;
 }
 
 // Pass 1: one thread per visible (view, splat) item of the lists above.

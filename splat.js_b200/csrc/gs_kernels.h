@@ -70,6 +70,11 @@ struct RadixHistArgs {
   uint32_t* epoch;
 };
 
+#ifndef GS_SORT_ITEMS
+#define GS_SORT_ITEMS 16  // keys per thread of a onesweep block (256 threads)
+#endif
+constexpr int SORT_BLOCK_ENTRIES = 256 * GS_SORT_ITEMS;  // entries one onesweep block ranks
+
 struct OnesweepArgs {
   const void* keysIn;
   const uint32_t* valsIn;

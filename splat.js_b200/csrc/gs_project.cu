@@ -319,7 +319,6 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
   const int lane = threadIdx.x & 31;
   const int wbase = threadIdx.x & ~31;
   const uint32_t FULL = 0xFFFFFFFFu;
-  const uint32_t ltm = (1u << lane) - 1u;
   const bool valid = p < items;
   uint32_t v = 0, i = 0, x0 = 0, x1 = 0, y0 = 0, rr = 0, out = 0;
   bool test = false;

@@ -126,9 +126,6 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
     const int x = tx * RT + lx, y = ty * RT + ly;
     const bool inside = x < c.W && y < c.H;
     const float px = (float)x + 0.5f, py = (float)y + 0.5f;
-    // centre of the warp's pixel centres (8 wide, 4 high)
-    const float wcx = (float)(tx * RT + (wid % WPR) * 8) + 4.0f;
-    const float wcy = (float)(ty * RT + (wid / WPR) * 4) + 2.0f;
     const uint2 rg = a.ranges[gt];
     const uint32_t s = rg.x, e = rg.y;
     const size_t pix = (size_t)c.pixBase + (size_t)y * c.W + x;

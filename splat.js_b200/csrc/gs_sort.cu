@@ -9,7 +9,7 @@
 // entries leaves each tile's ids in exactly that order.
 //
 // Onesweep: one histogram kernel reads every key once and counts all digit
-// positions; each digit pass then ranks a 4096-entry block in shared memory
+// positions; each digit pass then ranks a block of entries in shared memory
 // (warp ballots give each key its rank among equal digits), publishes the
 // block's per-digit counts, and obtains the count of every earlier block by
 // decoupled look-back before scattering.  Blocks are claimed in order through
@@ -133,8 +133,9 @@ void launch_exclusive_scan(const uint32_t* in, uint64_t N, uint32_t* out, uint32
 // ---------------------------------------------------------------------------
 constexpr int RS_THREADS = 256;
 constexpr int RS_WARPS = RS_THREADS / 32;
-constexpr int RS_ITEMS = 16;
-constexpr int RS_TILE = RS_THREADS * RS_ITEMS;  // 4096 entries per block
+constexpr int RS_ITEMS = GS_SORT_ITEMS;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;  // entries per block
+static_assert(RS_TILE == SORT_BLOCK_ENTRIES, "look-back buffers are sized by SORT_BLOCK_ENTRIES");
 constexpr int RS_MAX_PASSES = 8;
 constexpr uint32_t FLAG_AGG = 1u, FLAG_INC = 2u;
 constexpr uint32_t LOOKBACK_SPIN_LIMIT = 1u << 22;

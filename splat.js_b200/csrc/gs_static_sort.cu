@@ -30,7 +30,7 @@ namespace gs {
 namespace {
 
 constexpr uint32_t SS_MAX = GS_STATIC_SORT_MAX;
-constexpr uint32_t SS_BLOCK = 4096;                        // entries per onesweep block
+constexpr uint32_t SS_BLOCK = SORT_BLOCK_ENTRIES;          // entries per onesweep block
 constexpr uint32_t SS_STATUS = (SS_MAX / SS_BLOCK + 2) * 256;  // look-back words (block x digit)
 constexpr uint32_t SS_HIST = 8 * 256;                      // digit histograms of up to 8 passes
 // small words: [0, 2048) histograms, [2048, 2056) block counters,

@@ -399,7 +399,7 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   GS_AL(h->vals[0], h->capacity);
   GS_AL(h->vals[1], h->capacity);
   GS_AL(h->small, (size_t)4096);
-  GS_AL(h->lbStatus, (size_t)(std::max<uint64_t>(h->capacity, (uint64_t)B * cap) / 4096 + 2) * 256);
+  GS_AL(h->lbStatus, (size_t)(std::max<uint64_t>(h->capacity, (uint64_t)B * cap) / SORT_BLOCK_ENTRIES + 2) * 256);
   GS_AL(h->scanPartials, (size_t)scan_partials_needed((uint64_t)B * cap) + 1);
   GS_AL(h->outImg, (size_t)B * h->maxPix);
   GS_AL(h->finalT, (size_t)B * h->maxPix);
@@ -428,7 +428,7 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   }
   GS_CK(cudaMemsetAsync(h->gradP, 0, (size_t)B * cap * GP_STRIDE * 4, s));
   GS_CK(cudaMemsetAsync(h->small, 0, 4096 * 4, s));
-  GS_CK(cudaMemsetAsync(h->lbStatus, 0, (size_t)(std::max<uint64_t>(h->capacity, (uint64_t)B * cap) / 4096 + 2) * 256 * 8, s));
+  GS_CK(cudaMemsetAsync(h->lbStatus, 0, (size_t)(std::max<uint64_t>(h->capacity, (uint64_t)B * cap) / SORT_BLOCK_ENTRIES + 2) * 256 * 8, s));
   GS_CK(cudaMemcpyAsync(h->targets, packed.data(), std::max<uint64_t>(total, 4) * 4, cudaMemcpyHostToDevice, s));
   GS_CK(cudaMemsetAsync(h->stats, 0, 16, s));
   GS_CK(cudaMemsetAsync(h->gradCam, 0, (size_t)(ncams + 1) * 32, s));
