@@ -372,15 +372,27 @@ def run_ours(args):
         step_uneven(k)
     uneven_ms, uneven_vps = timed(step_uneven, args.steps, len(extra))
     # ---- end to end through the public API: per step the camera/Adam records
-    # go host->device from pinned memory and the loss statistics come back ----
+    # go host->device from pinned memory and the loss statistics come back to
+    # pinned host memory (readLoss, a Promise in the reference: the copy is
+    # enqueued each step and complete when the timed region's sync returns);
+    # the blocking variant (one host sync per step) is reported beside it ----
     st = (C.c_uint32 * 4)()
+    st_pinned = torch.zeros((max(args.steps, args.warmup), 4), dtype=torch.int32, pin_memory=True)
 
     def step_e2e(k):
+        step_batched(k)
+        N.check(L.gs_read_stats_async(h, C.c_void_p(st_pinned[k].data_ptr())), h)
+
+    def step_e2e_sync(k):
         step_batched(k)
         N.check(L.gs_read_stats(h, st), h)
     for k in range(args.warmup):
         step_e2e(k)
     e2e_ms, e2e_vps = timed(step_e2e, args.steps, B)
+    N.check(L.gs_sync(h), h)
+    for k in range(args.warmup):
+        step_e2e_sync(k)
+    e2e_sync_ms, e2e_sync_vps = timed(step_e2e_sync, args.steps, B)
     # ---- per-phase profile of the batched step (CUDA events on the stream) ----
     prof_steps = min(args.steps, 5)
     N.check(L.gs_profile(h, 1), h)
@@ -436,7 +448,10 @@ def run_ours(args):
                 "batched_vs_plain": batch_vps / plain_vps,
                 "uneven_batch": {"views": [f"{w}x{hh}" for w, hh in uneven_res], "views_per_s": uneven_vps,
                                  "ms_per_step": uneven_ms / args.steps},
-                "e2e": {"value": e2e_vps, "unit": "views/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 16},
+                "e2e": {"value": e2e_vps, "unit": "views/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 16,
+                        "read": "gs_read_stats_async into pinned memory each step (readLoss as a Promise)"},
+                "e2e_blocking_read": {"value": e2e_sync_vps, "unit": "views/s",
+                                      "read": "gs_read_stats each step (one host sync per step)"},
                 "gpu_launches": None,
                 "phases_ms_per_step": phase,
                 "pairs_per_step": pairs_per_launch,

@@ -147,6 +147,12 @@ GS_API int gs_step_batch(gs_trainer* h, const uint32_t* ci, uint32_t nviews);
 /* readLoss (trainer.js:615-631): copies and resets stats[4] = {SSE*16,
  * Charbonnier*32768, valid px, dropped tiles}; resets pixelsSeen. */
 GS_API int gs_read_stats(gs_trainer* h, uint32_t stats[4]);
+/* readLoss as the reference uses it, a Promise (trainer.js:615-631): enqueues
+ * the copy of stats[4] into `stats` (pinned host memory, else the copy is
+ * synchronous) and the reset, and returns at once; the values are valid after
+ * gs_sync.  Status bits and dropped-tile totals are checked at that sync by
+ * the caller (gs_sync reports device faults). */
+GS_API int gs_read_stats_async(gs_trainer* h, uint32_t* stats);
 /* readGaussians (trainer.js:797-817): params n*16, sh n*3K (either may be NULL). */
 GS_API int gs_read_gaussians(gs_trainer* h, float* params, float* sh, uint32_t* n);
 /* Overwrite the first n splats' parameters / SH (the parameter pokes of

@@ -906,6 +906,16 @@ int gs_read_stats(gs_trainer* h, uint32_t out[4]) {
   return check_status(h);
 }
 
+int gs_read_stats_async(gs_trainer* h, uint32_t* out) {
+  if (!h || !out) return GS_E_INVALID;
+  if (!h->ready) return fail(h, GS_E_INVALID, "setup() first");
+  cudaSetDevice(h->device);
+  GS_CK(cudaMemcpyAsync(out, h->stats, 16, cudaMemcpyDeviceToHost, h->stream));
+  GS_CK(cudaMemsetAsync(h->stats, 0, 16, h->stream));
+  h->pixelsSeen = 0;
+  return GS_OK;
+}
+
 int gs_read_gaussians(gs_trainer* h, float* params, float* sh, uint32_t* n) {
   if (!h) return GS_E_INVALID;
   if (!h->ready) return fail(h, GS_E_INVALID, "setup() first");

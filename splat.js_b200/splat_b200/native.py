@@ -87,6 +87,7 @@ def lib():
         "gs_step": (C.c_int, [H, C.c_uint32]),
         "gs_step_batch": (C.c_int, [H, u32p, C.c_uint32]),
         "gs_read_stats": (C.c_int, [H, u32p]),
+        "gs_read_stats_async": (C.c_int, [H, C.c_void_p]),
         "gs_read_gaussians": (C.c_int, [H, f32p, f32p, u32p]),
         "gs_write_gaussians": (C.c_int, [H, f32p, f32p, C.c_uint32]),
         "gs_read_moments": (C.c_int, [H, f32p, f32p, f32p, f32p]),

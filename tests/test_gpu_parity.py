@@ -445,3 +445,27 @@ def test_lookback_timeout_is_reported_and_device_stays_usable():
     assert st.value & 1, st.value
     assert ms.value < 5000.0, ms.value
     test_gradcheck_rig_raster_bitexact()
+
+
+def test_async_stats_read_matches_blocking_read():
+    """gs_read_stats_async (readLoss as a Promise) delivers the same stats as
+    the blocking read once the stream is synchronised."""
+    import ctypes as C
+    import torch
+    from splat_b200 import native as N
+    params, sh, cams, rgbs = config0()
+    got = []
+    for mode in ("sync", "async"):
+        t, targets, metas = make(params, sh, [dict(c) for c in cams], rgbs, dict(shDeg=2), radius=1.0)
+        t.iter = 2000
+        t.stepBatch([0])
+        if mode == "sync":
+            st = (C.c_uint32 * 4)()
+            N.check(N.lib().gs_read_stats(t._h, st), t._h)
+            got.append(list(st))
+        else:
+            buf = torch.zeros(4, dtype=torch.int32, pin_memory=True)
+            N.check(N.lib().gs_read_stats_async(t._h, C.c_void_p(buf.data_ptr())), t._h)
+            N.check(N.lib().gs_sync(t._h), t._h)
+            got.append([int(x) & 0xFFFFFFFF for x in buf.tolist()])
+    assert got[0] == got[1] and got[0][2] > 0, got
