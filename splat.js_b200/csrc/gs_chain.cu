@@ -278,18 +278,30 @@ __global__ void __launch_bounds__(128, GS_CHAIN_MIN_BLOCKS) k_chain_view(ChainAr
   const bool have = pos < cnt;
   const uint32_t i = have ? a.visList[(size_t)v * a.n + pos] : 0u;
   const int lane = threadIdx.x & 31;
-  // the block's camera in shared memory: read once, not re-fetched from
-  // global memory around every store
+  // the block's camera in shared memory (read once, not re-fetched from
+  // global memory around every store); every thread issues its own loads
+  // before the barrier that publishes it
   __shared__ DevCam s_cam;
   if (threadIdx.x == 0) s_cam = a.cams[v];
+  const size_t slot = (size_t)v * a.n + i;
+  int4 q0 = make_int4(0, 0, 0, 0), q1 = q0, q2 = q0;
+  float P[16];
+  if (have) {
+    const int4* G4 = reinterpret_cast<const int4*>(a.gradP + slot * GP_STRIDE);
+    q0 = G4[0]; q1 = G4[1]; q2 = G4[2];
+    const float4* P4 = reinterpret_cast<const float4*>(a.params + (size_t)i * STRIDE);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float4 t = __ldg(P4 + k);
+      P[4 * k] = t.x; P[4 * k + 1] = t.y; P[4 * k + 2] = t.z; P[4 * k + 3] = t.w;
+    }
+  }
   __syncthreads();
   const DevCam& c = s_cam;
   CamGrad7 cg = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f};
   if (have) {
-    const size_t slot = (size_t)v * a.n + i;
     {
       int4* G4 = reinterpret_cast<int4*>(a.gradP + slot * GP_STRIDE);
-      const int4 q0 = G4[0], q1 = G4[1], q2 = G4[2];
       G4[0] = make_int4(0, 0, 0, 0);
       G4[1] = make_int4(0, 0, 0, 0);
       G4[2] = make_int4(0, 0, 0, 0);
@@ -297,13 +309,6 @@ __global__ void __launch_bounds__(128, GS_CHAIN_MIN_BLOCKS) k_chain_view(ChainAr
       float gp[10];
 #pragma unroll
       for (int k = 0; k < 10; ++k) gp[k] = (float)qi[k] / ((k >= 2 && k <= 4) ? FIXEDC : FIXED);
-      float P[16];
-      const float4* P4 = reinterpret_cast<const float4*>(a.params + (size_t)i * STRIDE);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const float4 t = __ldg(P4 + k);
-        P[4 * k] = t.x; P[4 * k + 1] = t.y; P[4 * k + 2] = t.z; P[4 * k + 3] = t.w;
-      }
       float gF[16];
 #pragma unroll
       for (int k = 0; k < 16; ++k) gF[k] = 0.0f;
