@@ -32,18 +32,21 @@ template <int DEG>
 __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
   constexpr int K = DEG > 0 ? (DEG + 1) * (DEG + 1) - 1 : 0;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  // the batch's cameras in shared memory (read once per block)
+  // the batch's cameras in shared memory (read once per block); each thread
+  // issues its parameter loads before the barrier that publishes them
   __shared__ DevCam s_cams[MAX_VIEWS];
   for (int k = threadIdx.x; k < a.V; k += blockDim.x) s_cams[k] = a.cams[k];
+  float P[16];
+  if (i < a.n) {
+    const float4* P4 = reinterpret_cast<const float4*>(a.params + (size_t)i * STRIDE);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float4 t = P4[k];
+      P[4 * k] = t.x; P[4 * k + 1] = t.y; P[4 * k + 2] = t.z; P[4 * k + 3] = t.w;
+    }
+  }
   __syncthreads();
   if (i >= a.n) return;
-  float P[16];
-  const float4* P4 = reinterpret_cast<const float4*>(a.params + (size_t)i * STRIDE);
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const float4 t = P4[k];
-    P[4 * k] = t.x; P[4 * k + 1] = t.y; P[4 * k + 2] = t.z; P[4 * k + 3] = t.w;
-  }
   const float* shp = K > 0 ? a.sh + (size_t)i * 3 * K : nullptr;
   const float sig0 = sigm(P[10]), sig1 = sigm(P[11]), sig2 = sigm(P[12]);
   const float opa = sigm(P[13]);
