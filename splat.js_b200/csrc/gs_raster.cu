@@ -110,16 +110,13 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
   if (BWD)
     for (int k = tid; k < BATCH * 10; k += RTHREADS) s_acc[k] = 0;
 
-  // work items (global tiles of the batch): the next one is claimed while
-  // the current one is rendered, so the queue's atomic is off the critical path
-  if (tid == 0) s_item = a.workCounter ? atomicAdd(a.workCounter, 1u) : blockIdx.x;
-  __syncthreads();
-  for (;;) {
+  for (uint32_t iter = 0;; ++iter) {
+    // ---- next work item (a global tile of the batch) ----
+    if (tid == 0) s_item = a.workCounter ? atomicAdd(a.workCounter, 1u) : (iter == 0 ? blockIdx.x : 0xFFFFFFFFu);
+    __syncthreads();
     const uint32_t item = s_item;
     __syncthreads();
     if (item >= a.totalTiles) break;
-    uint32_t nextItem = 0xFFFFFFFFu;
-    if (tid == 0 && a.workCounter) nextItem = atomicAdd(a.workCounter, 1u);
     const uint32_t gt = a.workOrder ? a.workOrder[item] : item;
     int v = 0;
     while (v + 1 < a.V && a.cams[v + 1].tileBase <= gt) ++v;
@@ -390,8 +387,6 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
         hi = lo;
       }
     }
-    __syncthreads();
-    if (tid == 0) s_item = nextItem;
     __syncthreads();
   }
 }
