@@ -17,7 +17,7 @@ struct ProjectArgs {
   float eCut, aMin, radClamp;
   int tile;
   RenderRec* recs;         // V * n
-  uint64_t* pkeys;         // V * n presort keys: view << 32 | depth bits (all ones when culled)
+  uint32_t* pkeys;         // V * n presort keys: depth bits (all ones when culled)
   uint32_t* pvals;         // V * n presort values: slot = view * n + splat
   uint2* rect;             // V * n
   int32_t* diffGrid;       // per view (tilesX+1)*(tilesY+1), cleared before

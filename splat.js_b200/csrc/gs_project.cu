@@ -6,21 +6,22 @@
 // pairs into per-tile segments with atomic cursors and bitonic-sorts each
 // segment by (depth f32 bits, id) (shaders.js:303-500).  Here:
 //   1. k_project writes, per (view, splat), the raster record, the tile
-//      rectangle, four atomics into the view's tile difference grid (its 2D
-//      prefix sum is the reference's per-tile count), and a presort item:
-//      key (view << 32 | depth bits) -- all ones when culled -- and value
-//      slot = view * n + splat;
+//      rectangle, cull parameters, four atomics into the view's tile
+//      difference grid (its 2D prefix sum is the reference's per-tile
+//      count), and a presort item: key = depth bits -- all ones when culled
+//      -- and value slot = view * n + splat;
 //   2. k_tile_counts (one block per view): tileCnt, the reference's entry
 //      budget (drops), and view-local tile ranges; k_tile_ranges_finish
 //      offsets them by the earlier views' totals;
-//   3. the items are radix-sorted by key (stable, so equal depths keep id
-//      order): (view, depth, id) order;
-//   4. k_splat_counts / scan / k_keygen expand the sorted items into one
-//      entry per (splat, tile) -- key = global tile id (32 bits), value =
-//      splat id -- written in that order;
-//   5. a stable radix sort on the tile id leaves every tile's entries in
-//      (depth bits, id) order: the reference's per-tile order, with two
-//      passes over 8-byte entries instead of six over 12-byte ones.
+//   3. the items are radix-sorted by depth bits (stable from slot order, so
+//      equal depths keep id order; views stay interleaved);
+//   4. k_expand (count pass) / scan / k_expand (key pass) expand the sorted
+//      items into one entry per (splat, live tile) -- key = global tile id
+//      (32 bits), value = splat id -- written in that order;
+//   5. a stable radix sort on the global tile id (each id belongs to one
+//      view) leaves every tile's entries in (depth bits, id) order: the
+//      reference's per-tile order, with two passes over 8-byte entries
+//      instead of six over 12-byte ones.
 #include "gs_geom.cuh"
 #include "gs_kernels.h"
 
@@ -55,7 +56,7 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
     const DevCam& c = s_cams[v];
     const size_t slot = (size_t)v * a.n + i;
     a.rect[slot] = make_uint2(0xFFFFFFFFu, 0u);
-    a.pkeys[slot] = ~0ull;
+    a.pkeys[slot] = 0xFFFFFFFFu;
     a.pvals[slot] = (uint32_t)slot;
     const Geom g = computeGeom(c, P);
     if (!g.ok) continue;
@@ -109,7 +110,7 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
     r.r1 = make_float4(0.5f * (ad * inv), opa * comp, col[0], col[1]);
     r.r2 = make_float4(col[2], opa, -0.5f * cnorm, 1.0f - opa);
     a.recs[slot] = r;
-    a.pkeys[slot] = ((unsigned long long)v << 32) | __float_as_uint(g.pc[2]);
+    a.pkeys[slot] = __float_as_uint(g.pc[2]);  // positive: bit order = numeric order
 
     // tile bounds (shaders.js:303-308)
     const int tx = c.tilesX, ty = c.tilesY;

@@ -90,7 +90,7 @@ struct gs_trainer {
   uint32_t* workOrder = nullptr;
   uint32_t* keys[2] = {nullptr, nullptr};     // entries: global tile id
   uint32_t* vals[2] = {nullptr, nullptr};     // entries: splat id
-  uint64_t* pkeys[2] = {nullptr, nullptr};    // presort items: view << 32 | depth bits
+  uint64_t* pkeys[2] = {nullptr, nullptr};    // presort keys (u32 depth bits); refine's u64 donor keys
   uint32_t* pvals[2] = {nullptr, nullptr};    // presort items: slot = view * n + splat
   uint32_t* viewTotal = nullptr;
   uint64_t capacity = 0;
@@ -577,7 +577,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   pa.radClamp = h->o.radClamp;
   pa.tile = sh.tile;
   pa.recs = h->recs;
-  pa.pkeys = h->pkeys[0];
+  pa.pkeys = reinterpret_cast<uint32_t*>(h->pkeys[0]);
   pa.pvals = h->pvals[0];
   pa.rect = h->rect;
   pa.diffGrid = h->diffGrid;
@@ -600,21 +600,23 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   ta.totalEntries = totalEntries;
   launch_tile_ranges(ta, totalTiles, s);
 
-  // presort of the (view, splat) items by (view, depth): 4 byte digits of
-  // depth, one more for the view index when the batch has several views
+  // presort of the (view, splat) items by depth: 4 byte digits of the depth
+  // bits, stable from slot order, so equal depths stay in splat order.  Views
+  // stay interleaved: the tile sort groups entries by global tile id (which
+  // belongs to one view) and keeps this order inside every tile.
   uint32_t* nItems = h->small + 2061;
   cudaMemcpyAsync(nItems, &h->dParams->itemCount, 4, cudaMemcpyDeviceToDevice, s);
   RadixSortArgs pr{};
   pr.keys[0] = h->pkeys[0]; pr.keys[1] = h->pkeys[1];
   pr.vals[0] = h->pvals[0]; pr.vals[1] = h->pvals[1];
-  pr.keyBytes = 8;
+  pr.keyBytes = 4;
   pr.nItems = nItems;
   pr.hist = hist;
   pr.tileCounter = tileCounter;
   pr.status = h->lbStatus;
   pr.statusWord = statusWord;
   pr.epoch = epoch;
-  pr.passes = V > 1 ? 5 : 4;
+  pr.passes = 4;
   pr.keepKeys = false;
   pr.histGrid = (unsigned)h->histGrid;
   pr.sweepGrid = (unsigned)h->sweepGrid;
