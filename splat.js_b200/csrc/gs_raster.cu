@@ -305,15 +305,11 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
           uint32_t word = haveBits ? wmask[w] : FULL;
           if (wb + 32u > hi) word &= FULL >> (wb + 32u - hi);
           if (wb < lo) word &= FULL << (lo - wb);
-          // the word's records and accumulators, indexed by bit (entries below
-          // lo are masked off above, so bit + wb - lo is never negative when used)
-          const RenderRec* wrec = s_rec + ((int32_t)wb - (int32_t)lo);
-          int32_t* wacc = s_acc + ((int32_t)wb - (int32_t)lo) * 10;
           while (word) {
             const uint32_t bit = 31u - (uint32_t)__clz(word);
             word &= ~(1u << bit);
             const uint32_t j = wb + bit;
-            const RenderRec& rr = wrec[bit];
+            const RenderRec& rr = s_rec[j - lo];
             const float4 r0 = rr.r0;
             const float4 r1 = rr.r1;
             const float4 r2 = rr.r2;
@@ -367,16 +363,15 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
               S2 = __fmaf_rn(r2.x, aT, S2);
               Ta = Tb;
             }
-            // the 10 warp sums (equal in every lane) are staged by all lanes
-            // writing the same words, then lanes 0-9 add one each
-            {
+            // lane 0 stages the 10 warp sums; lanes 0-9 add one each
+            if (lane == 0) {
               int4* st = reinterpret_cast<int4*>(s_stage[wid]);
               st[0] = make_int4((int)rsum[0], (int)rsum[1], (int)rsum[2], (int)rsum[3]);
               st[1] = make_int4((int)rsum[4], (int)rsum[5], (int)rsum[6], (int)rsum[7]);
               reinterpret_cast<int2*>(s_stage[wid])[4] = make_int2((int)rsum[8], (int)rsum[9]);
             }
             __syncwarp();
-            if (lane < 10) atomicAdd(&wacc[bit * 10 + (uint32_t)lane], s_stage[wid][lane]);
+            if (lane < 10) atomicAdd(&s_acc[(j - lo) * 10 + (uint32_t)lane], s_stage[wid][lane]);
             __syncwarp();
           }
         }
