@@ -154,6 +154,14 @@ GS_API int gs_read_stats(gs_trainer* h, uint32_t stats[4]);
  * the caller (gs_sync reports device faults). */
 GS_API int gs_read_stats_async(gs_trainer* h, uint32_t* stats);
 /* readGaussians (trainer.js:797-817): params n*16, sh n*3K (either may be NULL). */
+/* PLY export: bakeOpacityCompensation (ply.js:17-39; bake = 0 skips it, f the
+ * focal length, camPositions ncams xyz JavaScript numbers) followed by
+ * gaussiansToPly (ply.js:45-99) of the current Gaussians (with SH when
+ * shDeg > 0), computed on the device in double precision as the JavaScript
+ * does.  Writes the binary PLY (text header + n records) to out; out = NULL
+ * only reports the size in *size; cap < size gives GS_E_LIMIT. */
+GS_API int gs_export_ply(gs_trainer* h, int32_t bake, double f, const double* camPositions, uint32_t ncams,
+                         uint8_t* out, uint64_t cap, uint64_t* size);
 GS_API int gs_read_gaussians(gs_trainer* h, float* params, float* sh, uint32_t* n);
 /* Overwrite the first n splats' parameters / SH (the parameter pokes of
  * gradcheck.js:320-323; either pointer may be NULL). */

@@ -262,3 +262,47 @@ def adam(hp, n, K, params, gradF, m, v, sh, shGrad, shM, shV):
     lib().oracle_adam_f32(C.byref(hp), n, K, _p(params, C.c_float), _p(gradF, C.c_float), _p(m, C.c_float),
                           _p(v, C.c_float), _p(sh, C.c_float), _p(shGrad, C.c_float), _p(shM, C.c_float),
                           _p(shV, C.c_float))
+
+
+def ply_export(params, n, sh=None, shK=0, bake=False, f=0.0, cam_positions=()):
+    """ply.js:17-99 restated in numpy (double precision, float32 stores):
+    bakeOpacityCompensation (when bake) followed by gaussiansToPly.  Returns
+    the PLY bytes."""
+    P = np.asarray(params, np.float32).reshape(-1, 16)[:n].astype(np.float64)
+    K = shK if sh is not None else 0
+    logit = P[:, 13].copy()
+    if bake:
+        cams = np.asarray(cam_positions, np.float64).reshape(-1, 3)
+        z2min = np.full(n, np.inf)
+        for c in cams:                                    # ply.js:22-29
+            d2 = (P[:, 0] - c[0]) * (P[:, 0] - c[0]) + (P[:, 1] - c[1]) * (P[:, 1] - c[1]) \
+                + (P[:, 2] - c[2]) * (P[:, 2] - c[2])
+            z2min = np.minimum(z2min, d2)
+        z = np.maximum(1e-3, np.sqrt(z2min))
+        s_mean = np.exp((P[:, 3] + P[:, 4] + P[:, 5]) / 3)
+        s2d = f * s_mean / z
+        comp = (s2d * s2d) / (s2d * s2d + 0.3)
+        opa = comp / (1 + np.exp(-P[:, 13]))
+        cl = np.minimum(1 - 1e-6, np.maximum(1e-6, opa))
+        logit = np.log(cl / (1 - cl)).astype(np.float32).astype(np.float64)
+    props = ['x', 'y', 'z', 'nx', 'ny', 'nz', 'f_dc_0', 'f_dc_1', 'f_dc_2'] + \
+        [f'f_rest_{k}' for k in range(3 * K)] + \
+        ['opacity', 'scale_0', 'scale_1', 'scale_2', 'rot_0', 'rot_1', 'rot_2', 'rot_3']
+    header = 'ply\nformat binary_little_endian 1.0\n' + f'element vertex {n}\n' + \
+        '\n'.join(f'property float {p}' for p in props) + '\nend_header\n'
+    rec = np.zeros((n, len(props)), np.float32)
+    rec[:, 0:3] = P[:, 0:3]
+    sig = 1 / (1 + np.exp(-P[:, 10:13]))
+    rec[:, 6:9] = (sig - 0.5) / 0.28209479177387814
+    if K:
+        rec[:, 9:9 + 3 * K] = np.asarray(sh, np.float32).reshape(-1, 3 * K)[:n]
+    q0 = 9 + 3 * K
+    rec[:, q0] = logit
+    rec[:, q0 + 1:q0 + 4] = P[:, 3:6]
+    q = P[:, 6:10].copy()
+    ql = np.sqrt((q * q).sum(1))
+    small = ql < 1e-6
+    q[~small] = q[~small] / ql[~small, None]
+    q[small] = [1.0, 0.0, 0.0, 0.0]
+    rec[:, q0 + 4:q0 + 8] = q
+    return header.encode() + rec.astype('<f4').tobytes()

@@ -194,6 +194,8 @@ uint32_t scan_partials_needed(uint64_t N);
 void launch_exclusive_scan(const uint32_t* in, uint64_t N, uint32_t* out, uint32_t* partials, uint32_t* total,
                            cudaStream_t s);
 int onesweep_grid(int device);
+int export_ply_records(const float* params, const float* sh, uint32_t n, uint32_t K, int bake, double f,
+                       const double* camPosHost, uint32_t ncams, float* outHost, cudaStream_t s);
 int debug_lookback_timeout(int device, uint32_t spinLimit, uint32_t* statusOut, double* msOut);
 void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s);
 void launch_raster(const RasterArgs& a, int mode, bool stored, int tile, int batchDepth, unsigned grid,

@@ -918,6 +918,34 @@ int gs_read_stats_async(gs_trainer* h, uint32_t* out) {
   return GS_OK;
 }
 
+int gs_export_ply(gs_trainer* h, int32_t bake, double f, const double* camPositions, uint32_t ncams, uint8_t* out,
+                  uint64_t cap, uint64_t* size) {
+  if (!h || !size) return GS_E_INVALID;
+  if (!h->ready) return fail(h, GS_E_INVALID, "setup() first");
+  if (bake && ncams && !camPositions) return fail(h, GS_E_INVALID, "camPositions is NULL");
+  // header of gaussiansToPly (ply.js:51-69)
+  std::string hdr = "ply\nformat binary_little_endian 1.0\nelement vertex " + std::to_string(h->n) + "\n";
+  const char* head[] = {"x", "y", "z", "nx", "ny", "nz", "f_dc_0", "f_dc_1", "f_dc_2"};
+  for (const char* p : head) hdr += std::string("property float ") + p + "\n";
+  for (uint32_t k = 0; k < 3 * h->K; ++k) hdr += "property float f_rest_" + std::to_string(k) + "\n";
+  const char* tail[] = {"opacity", "scale_0", "scale_1", "scale_2", "rot_0", "rot_1", "rot_2", "rot_3"};
+  for (const char* p : tail) hdr += std::string("property float ") + p + "\n";
+  hdr += "end_header\n";
+  const uint64_t body = (uint64_t)h->n * (17 + 3 * h->K) * 4;
+  *size = hdr.size() + body;
+  if (!out) return GS_OK;
+  if (cap < *size) return fail(h, GS_E_LIMIT, "output buffer smaller than the PLY");
+  cudaSetDevice(h->device);
+  std::memcpy(out, hdr.data(), hdr.size());
+  std::vector<float> rec((size_t)h->n * (17 + 3 * h->K));
+  const int rc = export_ply_records(h->params, h->K ? h->sh : nullptr, h->n, h->K, bake, f, camPositions, ncams,
+                                    rec.data(), h->stream);
+  if (rc == -3) return fail(h, GS_E_NOMEM, "PLY export buffers");
+  if (rc) return fail(h, GS_E_CUDA, "PLY export kernel");
+  std::memcpy(out + hdr.size(), rec.data(), body);
+  return GS_OK;
+}
+
 int gs_read_gaussians(gs_trainer* h, float* params, float* sh, uint32_t* n) {
   if (!h) return GS_E_INVALID;
   if (!h->ready) return fail(h, GS_E_INVALID, "setup() first");

@@ -89,6 +89,8 @@ def lib():
         "gs_read_stats": (C.c_int, [H, u32p]),
         "gs_read_stats_async": (C.c_int, [H, C.c_void_p]),
         "gs_read_gaussians": (C.c_int, [H, f32p, f32p, u32p]),
+        "gs_export_ply": (C.c_int, [H, C.c_int32, C.c_double, P(C.c_double), C.c_uint32, C.c_void_p, C.c_uint64,
+                                    u64p]),
         "gs_write_gaussians": (C.c_int, [H, f32p, f32p, C.c_uint32]),
         "gs_read_moments": (C.c_int, [H, f32p, f32p, f32p, f32p]),
         "gs_render": (C.c_int, [H, P(GsCamera), C.c_int32, C.c_uint32, f32p]),

@@ -469,3 +469,36 @@ def test_async_stats_read_matches_blocking_read():
             N.check(N.lib().gs_sync(t._h), t._h)
             got.append([int(x) & 0xFFFFFFFF for x in buf.tolist()])
     assert got[0] == got[1] and got[0][2] > 0, got
+
+
+@pytest.mark.parametrize("bake", [False, True])
+def test_ply_export_matches_ply_js_restatement(bake):
+    """gs_export_ply (bakeOpacityCompensation + gaussiansToPly on the device)
+    against a numpy restatement of ply.js: identical header and layout, every
+    float within one float32 ulp (JavaScript/CUDA/numpy double exp, log and
+    square root agree to a double ulp before the float32 store)."""
+    import ctypes as C
+    from splat_b200 import native as N
+    params, sh, cams, rgbs = config0(n=5000, seed=4)
+    t, targets, metas = make(params, sh, [dict(c) for c in cams], rgbs, dict(shDeg=2), radius=1.0)
+    t.iter = 2000
+    t.stepBatch([0])
+    t.stepBatch([0])
+    g = t.readGaussians()
+    campos = np.array([[0.0, 0.0, -3.0], [1.0, 0.5, -2.5], [-2.0, 0.1, 0.3]], np.float64)
+    size = C.c_uint64()
+    L = N.lib()
+    N.check(L.gs_export_ply(t._h, int(bake), 300.0, campos.ctypes.data_as(C.POINTER(C.c_double)), 3, None, 0,
+                            C.byref(size)), t._h)
+    out = np.zeros(size.value, np.uint8)
+    N.check(L.gs_export_ply(t._h, int(bake), 300.0, campos.ctypes.data_as(C.POINTER(C.c_double)), 3,
+                            C.c_void_p(out.ctypes.data), size.value, C.byref(size)), t._h)
+    ref = O.ply_export(g["data"], g["n"], g["sh"], g["shK"], bake=bake, f=300.0, cam_positions=campos)
+    got = out.tobytes()
+    hlen = ref.index(b"end_header\n") + len(b"end_header\n")
+    assert got[:hlen] == ref[:hlen]
+    a = np.frombuffer(got[hlen:], "<i4")
+    b = np.frombuffer(ref[hlen:], "<i4")
+    assert a.size == b.size
+    ulp = np.abs(a.astype(np.int64) - b.astype(np.int64))
+    assert ulp.max() <= 1, (int(ulp.max()), int((ulp > 0).sum()))
