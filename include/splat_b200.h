@@ -206,6 +206,10 @@ GS_API int gs_profile_read(gs_trainer* h, double ms[4], uint32_t launches[4]);
 /* FP32 FMA throughput of device `device` in TFLOP/s (an FFMA-chain kernel),
  * the peak the raster kernels' roofline is quoted against. */
 GS_API int gs_probe_fp32_peak(int32_t device, double* tflops);
+/* Check of the rasteriser's reciprocal of 1 - alpha (no reference
+ * counterpart): compares it with IEEE 1/x for every float x in [2^-7, 1];
+ * *mismatches must be 0 (*firstBits: the first failing x's bits). */
+GS_API int gs_debug_check_rcp(int32_t device, uint64_t* mismatches, uint32_t* firstBits);
 
 /* ---- allocation-free entry sort (no counterpart in the reference) ----
  * For callers that cannot call cudaMalloc: code whose device memory is owned

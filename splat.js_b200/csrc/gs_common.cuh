@@ -71,6 +71,21 @@ __device__ __forceinline__ float gexp(float x) {
   return __fmul_rn(p, __uint_as_float(sb));
 }
 
+// 1/x rounded to nearest (equal to IEEE 1.0f / x) for x in [2^-7, 1]: the
+// hardware's approximate reciprocal refined by two Newton-Raphson steps with
+// fused multiply-adds (e = 1 - x y; y += e y), the last of which acts as
+// Markstein's correction step.  The domain has no zeros, denormals or
+// infinities, so no slow path is needed; gs_debug_check_rcp compares the
+// result with IEEE division for every float in the domain.
+__device__ __forceinline__ float rcp_unit(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  float e = __fmaf_rn(-x, y, 1.0f);
+  y = __fmaf_rn(e, y, y);
+  e = __fmaf_rn(-x, y, 1.0f);
+  return __fmaf_rn(e, y, y);
+}
+
 // log(x), x positive normal: x = m 2^e, m in [sqrt(1/2), sqrt(2)),
 // log m = 2 atanh((m-1)/(m+1)) by its odd series to degree 11.
 __device__ __forceinline__ float glog(float x) {

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/splat_b200.h"
+#include "gs_common.cuh"
 
 namespace {
 
@@ -26,7 +27,42 @@ __global__ void __launch_bounds__(256) k_ffma(float* out, float a, float b) {
   if (s == 12345.678f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// every float in [lo, hi] (bit patterns): rcp_unit(x) against IEEE 1/x
+__global__ void k_check_rcp(uint32_t lo, uint32_t hi, unsigned long long* bad, uint32_t* first) {
+  for (uint32_t b = lo + blockIdx.x * blockDim.x + threadIdx.x; b <= hi; b += gridDim.x * blockDim.x) {
+    const float x = __uint_as_float(b);
+    if (__float_as_uint(gs::rcp_unit(x)) != __float_as_uint(__frcp_rn(x))) {
+      atomicAdd(bad, 1ull);
+      atomicMin(first, b);
+    }
+  }
+}
+
 }  // namespace
+
+extern "C" GS_API int gs_debug_check_rcp(int32_t device, uint64_t* mismatches, uint32_t* firstBits) {
+  if (!mismatches || !firstBits) return GS_E_INVALID;
+  if (cudaSetDevice(device) != cudaSuccess) return GS_E_CUDA;
+  unsigned long long* bad = nullptr;
+  uint32_t* first = nullptr;
+  if (cudaMalloc(&bad, 8) != cudaSuccess || cudaMalloc(&first, 4) != cudaSuccess) {
+    cudaFree(bad);
+    return GS_E_NOMEM;
+  }
+  cudaMemset(bad, 0, 8);
+  cudaMemset(first, 0xFF, 4);
+  k_check_rcp<<<1184, 256>>>(0x3C000000u, 0x3F800000u, bad, first);  // [2^-7, 1]
+  unsigned long long nb = 0;
+  uint32_t fb = 0;
+  const bool ok = cudaMemcpy(&nb, bad, 8, cudaMemcpyDeviceToHost) == cudaSuccess &&
+                  cudaMemcpy(&fb, first, 4, cudaMemcpyDeviceToHost) == cudaSuccess;
+  cudaFree(bad);
+  cudaFree(first);
+  if (!ok) return GS_E_CUDA;
+  *mismatches = nb;
+  *firstBits = fb;
+  return GS_OK;
+}
 
 extern "C" GS_API int gs_probe_fp32_peak(int32_t device, double* tflops) {
   if (!tflops) return GS_E_INVALID;

@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
             const float alpha = fminf(0.99f, araw);
             const bool c2 = j < myEnd && ee <= E_CUT && alpha >= A_MIN;
             if (!__any_sync(FULL, c2)) continue;
-            const float inv = __frcp_rn(1.0f - alpha);
+            const float inv = rcp_unit(1.0f - alpha);  // 1 - alpha in [0.01, 1]: IEEE 1/x exactly
             const float Tb = STORED ? (c2 ? a.tStore[(size_t)(s + j) * RTHREADS + tid] : 0.0f) : Ta * inv;
             const float aT = c2 ? alpha * Tb : 0.0f;
             const float g0 = __fmaf_rn(r1.z, Tb, -(S0 * inv));

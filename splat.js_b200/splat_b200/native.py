@@ -103,6 +103,7 @@ def lib():
         "gs_profile": (C.c_int, [H, C.c_int32]),
         "gs_profile_read": (C.c_int, [H, P(C.c_double), u32p]),
         "gs_probe_fp32_peak": (C.c_int, [C.c_int32, P(C.c_double)]),
+        "gs_debug_check_rcp": (C.c_int, [C.c_int32, u64p, u32p]),
         "gs_sort_entries_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]),
         "gs_autotune": (C.c_int, [H, u32p, C.c_uint32, C.c_int32, i32p, i32p, f32p]),
         "gs_set_raster_config": (C.c_int, [H, C.c_int32, C.c_int32]),

@@ -502,3 +502,13 @@ def test_ply_export_matches_ply_js_restatement(bake):
     assert a.size == b.size
     ulp = np.abs(a.astype(np.int64) - b.astype(np.int64))
     assert ulp.max() <= 1, (int(ulp.max()), int((ulp > 0).sum()))
+
+
+def test_unit_reciprocal_is_ieee_on_its_domain():
+    """The rasteriser's reciprocal of 1 - alpha equals IEEE 1/x for every
+    float in [2^-7, 1] (1 - alpha lies in [0.01, 1])."""
+    import ctypes as C
+    from splat_b200 import native as N
+    bad, first = C.c_uint64(), C.c_uint32()
+    N.check(N.lib().gs_debug_check_rcp(0, C.byref(bad), C.byref(first)), None)
+    assert bad.value == 0, (bad.value, hex(first.value))
