@@ -99,6 +99,7 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
   __shared__ uint32_t s_item;
   __shared__ uint32_t s_redu[NW][5];
   __shared__ uint32_t s_endmax[NW];
+  __shared__ __align__(16) int32_t s_stage[BWD ? NW : 1][12];  // per warp: the 10 sums of one entry
 
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int lx = (wid % WPR) * 8 + (lane & 7);
@@ -362,17 +363,16 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
               S2 = __fmaf_rn(r2.x, aT, S2);
               Ta = Tb;
             }
-            // the 10 warp sums are equal in every lane; lane k (k < 10) picks
-            // sum k with a select tree on its lane bits and adds it
-            {
-              const uint32_t v01 = (lane & 1) ? rsum[1] : rsum[0], v23 = (lane & 1) ? rsum[3] : rsum[2];
-              const uint32_t v45 = (lane & 1) ? rsum[5] : rsum[4], v67 = (lane & 1) ? rsum[7] : rsum[6];
-              const uint32_t v89 = (lane & 1) ? rsum[9] : rsum[8];
-              const uint32_t w03 = (lane & 2) ? v23 : v01, w47 = (lane & 2) ? v67 : v45;
-              const uint32_t x07 = (lane & 4) ? w47 : w03;
-              const uint32_t mine = (lane & 8) ? v89 : x07;
-              if (lane < 10) atomicAdd(&s_acc[(j - lo) * 10 + (uint32_t)lane], (int32_t)mine);
+            // lane 0 stages the 10 warp sums; lanes 0-9 add one each
+            if (lane == 0) {
+              int4* st = reinterpret_cast<int4*>(s_stage[wid]);
+              st[0] = make_int4((int)rsum[0], (int)rsum[1], (int)rsum[2], (int)rsum[3]);
+              st[1] = make_int4((int)rsum[4], (int)rsum[5], (int)rsum[6], (int)rsum[7]);
+              reinterpret_cast<int2*>(s_stage[wid])[4] = make_int2((int)rsum[8], (int)rsum[9]);
             }
+            __syncwarp();
+            if (lane < 10) atomicAdd(&s_acc[(j - lo) * 10 + (uint32_t)lane], s_stage[wid][lane]);
+            __syncwarp();
           }
         }
         __syncthreads();
