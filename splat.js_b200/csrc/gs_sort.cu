@@ -178,6 +178,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_onesweep(OnesweepArgs a) {
   KT* keysOut = static_cast<KT*>(a.keysOut);
   __shared__ uint32_t s_whist[RS_WARPS][256];
   __shared__ uint32_t s_count[256];     // this block's count per digit
+  __shared__ uint32_t s_run[256];       // the same, kept for the look-back
   __shared__ uint32_t s_local[256];     // exclusive prefix of s_count over digits
   __shared__ uint32_t s_gbase[256];     // global start of this block's run per digit
   __shared__ uint32_t s_dbase[256];     // exclusive scan of the pass histogram
@@ -279,37 +280,14 @@ __global__ void __launch_bounds__(RS_THREADS) k_onesweep(OnesweepArgs a) {
       }
       s_count[d] = run;
 
-      // decoupled look-back for digit d
+      // publish this block's count (the whole prefix for block 0) at once, so
+      // the blocks behind it can proceed while it stages its entries
       cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> my(
           *reinterpret_cast<unsigned long long*>(a.status + (size_t)tile * 256 + d));
-      uint32_t excl = 0;
-      if (tile == 0) {
-        my.store(((unsigned long long)tag << 32) | ((unsigned long long)FLAG_INC << 30) | run,
-                 cuda::memory_order_relaxed);
-      } else {
-        my.store(((unsigned long long)tag << 32) | ((unsigned long long)FLAG_AGG << 30) | run,
-                 cuda::memory_order_relaxed);
-        int64_t t = (int64_t)tile - 1;
-        uint32_t spins = 0;
-        while (t >= 0) {
-          cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> pr(
-              *reinterpret_cast<unsigned long long*>(a.status + (size_t)t * 256 + d));
-          const unsigned long long s = pr.load(cuda::memory_order_relaxed);
-          const uint32_t stag = (uint32_t)(s >> 32);
-          const uint32_t flag = (uint32_t)(s >> 30) & 3u;
-          if (stag != tag || flag == 0) {
-            if (++spins > a.spinLimit) { atomicOr(a.statusWord, ST_LOOKBACK_TIMEOUT); break; }
-            __nanosleep(32);
-            continue;
-          }
-          excl += (uint32_t)(s & 0x3FFFFFFFull);
-          if (flag == FLAG_INC) break;
-          --t;
-        }
-        my.store(((unsigned long long)tag << 32) | ((unsigned long long)FLAG_INC << 30) | (excl + run),
-                 cuda::memory_order_relaxed);
-      }
-      s_gbase[d] = s_dbase[d] + excl;
+      my.store(((unsigned long long)tag << 32) |
+                   ((unsigned long long)(tile == 0 ? FLAG_INC : FLAG_AGG) << 30) | run,
+               cuda::memory_order_relaxed);
+      s_run[d] = run;
     }
     // exclusive scan of s_count over digits -> s_local
     {
@@ -345,6 +323,38 @@ __global__ void __launch_bounds__(RS_THREADS) k_onesweep(OnesweepArgs a) {
         s_keys[pos] = key[j];
         s_vals[pos] = val[j];
       }
+    }
+    __syncthreads();
+    // decoupled look-back for digit d (the staged entries wait in shared
+    // memory, so no per-entry registers are held while it spins)
+    {
+      const int d = tid;
+      const uint32_t run = s_run[d];
+      cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> my(
+          *reinterpret_cast<unsigned long long*>(a.status + (size_t)tile * 256 + d));
+      uint32_t excl = 0;
+      if (tile != 0) {
+        int64_t t = (int64_t)tile - 1;
+        uint32_t spins = 0;
+        while (t >= 0) {
+          cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> pr(
+              *reinterpret_cast<unsigned long long*>(a.status + (size_t)t * 256 + d));
+          const unsigned long long sw = pr.load(cuda::memory_order_relaxed);
+          const uint32_t stag = (uint32_t)(sw >> 32);
+          const uint32_t flag = (uint32_t)(sw >> 30) & 3u;
+          if (stag != tag || flag == 0) {
+            if (++spins > a.spinLimit) { atomicOr(a.statusWord, ST_LOOKBACK_TIMEOUT); break; }
+            __nanosleep(32);
+            continue;
+          }
+          excl += (uint32_t)(sw & 0x3FFFFFFFull);
+          if (flag == FLAG_INC) break;
+          --t;
+        }
+        my.store(((unsigned long long)tag << 32) | ((unsigned long long)FLAG_INC << 30) | (excl + run),
+                 cuda::memory_order_relaxed);
+      }
+      s_gbase[d] = s_dbase[d] + excl;
     }
     __syncthreads();
     const uint32_t cnt = min((uint32_t)RS_TILE, N - base);
