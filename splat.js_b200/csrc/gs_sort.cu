@@ -166,11 +166,10 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 }
 
 template <typename KT>
-#ifdef GS_SORT_MIN_BLOCKS
-__global__ void __launch_bounds__(RS_THREADS, GS_SORT_MIN_BLOCKS) k_onesweep(OnesweepArgs a) {
-#else
-__global__ void __launch_bounds__(RS_THREADS) k_onesweep(OnesweepArgs a) {
+#ifndef GS_SORT_MIN_BLOCKS
+#define GS_SORT_MIN_BLOCKS 3  // resident blocks per SM the register allocation must allow
 #endif
+__global__ void __launch_bounds__(RS_THREADS, GS_SORT_MIN_BLOCKS) k_onesweep(OnesweepArgs a) {
   extern __shared__ __align__(16) unsigned char rs_dyn[];
   KT* s_keys = reinterpret_cast<KT*>(rs_dyn);                                    // RS_TILE keys
   uint32_t* s_vals = reinterpret_cast<uint32_t*>(rs_dyn + RS_TILE * sizeof(KT));  // RS_TILE values
