@@ -461,8 +461,8 @@ def run_ours(args):
                              "frac": achieved / peak.value if peak.value else None,
                              "traffic": RASTER_DRAM_BYTES_8VIEW if (B == 8 and n == 1_000_000 and args.width == 1920)
                              else None,
-                             "traffic_source": "ncu capture of one 8-view step (cameras 0-7), "
-                                               "profiles/raster_16x256_step8_1M_1080p.md",
+                             "traffic_source": "one ncu capture of the raster over an 8-view step (cameras 0-7) "
+                                               "of this workload",
                              "peak_source": "gs_probe_fp32_peak FFMA kernel on this GPU (measured)",
                              "work": f"{FLOP_PER_PAIR} flop per pixel-entry pair P of the reference's tile lists "
                                      "(pairs up to each pixel's termination index); the step walks culled lists "
