@@ -372,37 +372,22 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
 #pragma unroll
     for (int k = 0; k < SHN; ++k) shA[k] = 0.0f;
     if (i < a.n) {
-      // the views that saw this splat (rectangle loads issued together)
-      uint32_t vis = 0;
-#pragma unroll 4
-      for (int v = 0; v < a.V; ++v) vis |= (a.rect[(size_t)v * a.n + i].x != 0xFFFFFFFFu ? 1u : 0u) << v;
-      // views in order; the next view's results are loaded while this one is summed
-      const float4* q = nullptr;
-      float4 n0, n1, n2, n3, n4;
-      int v = vis ? __ffs(vis) - 1 : -1;
-      if (v >= 0) {
-        q = reinterpret_cast<const float4*>(a.viewGrad + ((size_t)v * a.n + i) * VIEWGRAD_STRIDE);
-        n0 = q[0]; n1 = q[1]; n2 = q[2]; n3 = q[3]; n4 = K > 0 ? q[4] : n3;
-      }
-      while (v >= 0) {
-        const float4 q0 = n0, q1 = n1, q2 = n2, q3 = n3, q4 = n4;
-        const int cv = v;
-        vis &= vis - 1u;
-        v = vis ? __ffs(vis) - 1 : -1;
-        if (v >= 0) {
-          q = reinterpret_cast<const float4*>(a.viewGrad + ((size_t)v * a.n + i) * VIEWGRAD_STRIDE);
-          n0 = q[0]; n1 = q[1]; n2 = q[2]; n3 = q[3]; n4 = K > 0 ? q[4] : n3;
-        }
+      for (int v = 0; v < a.V; ++v) {
+        const size_t slot = (size_t)v * a.n + i;
+        if (a.rect[slot].x == 0xFFFFFFFFu) continue;
+        const float4* q = reinterpret_cast<const float4*>(a.viewGrad + slot * VIEWGRAD_STRIDE);
+        const float4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
         const float gF[14] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w,
                               q2.x, q2.y, q2.z, q2.w, q3.x, q3.y};
 #pragma unroll
         for (int k = 0; k < 14; ++k) gFa[k] = gFa[k] + gF[k];
         if (K > 0) {
+          const float4 q4 = q[4];
           const float dRGB[3] = {q3.z, q3.w, q4.x};
           const float vd[3] = {q4.y, q4.z, q4.w};
           float Y[15];
           shBasis<DEG>(vd, Y);
-          const int aK = shActiveK(a.cams[cv], K);
+          const int aK = shActiveK(a.cams[v], K);
 #pragma unroll
           for (int ch = 0; ch < 3; ++ch)
 #pragma unroll
