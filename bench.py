@@ -87,23 +87,62 @@ def config_dict(args, extra=None):
 # clocks during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
+    """SM clock and clock-event reasons sampled during the timed region: NVML
+    in a thread every 10 ms (read-only queries), else nvidia-smi every 200 ms."""
     FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    # NVML clock-event reason bits
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                   "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
 
     def __init__(self, device):
         self.device = device
+        self.uuid = None
         self.p = None
+        self.samples = []
+        self.mx = None
+        self.reasons = set()
+        self._stop = None
+        self._thread = None
         try:
             import torch
-            self.device = "GPU-" + str(torch.cuda.get_device_properties(device).uuid)
+            self.uuid = "GPU-" + str(torch.cuda.get_device_properties(device).uuid)
         except Exception:
             pass
 
+    def _nvml_loop(self, handle, nv):
+        import time as _t
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(handle, nv.NVML_CLOCK_SM)))
+                try:
+                    bits = nv.nvmlDeviceGetCurrentClocksEventReasons(handle)
+                except AttributeError:
+                    bits = nv.nvmlDeviceGetCurrentClocksThrottleReasons(handle)
+                for nm, b in self.REASON_BITS.items():
+                    if bits & b:
+                        self.reasons.add(nm)
+            except Exception:
+                pass
+            _t.sleep(0.01)
+
     def __enter__(self):
         try:
+            import threading
+            import pynvml as nv
+            nv.nvmlInit()
+            handle = nv.nvmlDeviceGetHandleByUUID(self.uuid) if self.uuid else nv.nvmlDeviceGetHandleByIndex(0)
+            self.mx = float(nv.nvmlDeviceGetMaxClockInfo(handle, nv.NVML_CLOCK_SM))
+            self._stop = threading.Event()
+            self._thread = threading.Thread(target=self._nvml_loop, args=(handle, nv), daemon=True)
+            self._thread.start()
+            return self
+        except Exception:
+            self._thread = None
+        try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                       "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                       "-lms", "200", "-i", str(self.uuid or self.device)], stdout=subprocess.PIPE,
                                       stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.p = None
@@ -111,6 +150,9 @@ class ClockSampler:
 
     def __exit__(self, *a):
         self.out = ""
+        if self._thread:
+            self._stop.set()
+            self._thread.join(timeout=2)
         if self.p:
             self.p.terminate()
             try:
@@ -120,7 +162,7 @@ class ClockSampler:
                 self.out, _ = self.p.communicate()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
+        sm, mx, reasons = list(self.samples), self.mx, set(self.reasons)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in (self.out or "").splitlines():
             f = [x.strip() for x in line.split(",")]
@@ -136,7 +178,8 @@ class ClockSampler:
                     reasons.add(nm)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": ["unsampled"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml 10 ms" if self.samples else "nvidia-smi 200 ms"}
 
 
 # ---------------------------------------------------------------------------
@@ -457,6 +500,8 @@ def run_ours(args):
                 "pairs_per_step": pairs_per_launch,
                 "pairs_executed_per_step": pairs_exec,
                 "roofline": {"bound": "fp32", "kernel": "raster (fused forward + loss + backward)",
+                             "bound_note": "FP32 CUDA-core (issue) bound: no tensor-core or HBM bound applies; "
+                                           "the peak is this GPU's measured FFMA throughput",
                              "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                              "frac": achieved / peak.value if peak.value else None,
                              "traffic": RASTER_DRAM_BYTES_8VIEW if (B == 8 and n == 1_000_000 and args.width == 1920)
