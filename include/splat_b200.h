@@ -197,7 +197,8 @@ GS_API int gs_sync(gs_trainer* h);
  * that stream bracket the step. */
 GS_API int gs_set_stream(gs_trainer* h, void* stream);
 /* Per-phase CUDA-event timing: while enabled, steps run without graph replay
- * and each phase (0 project+count+keygen, 1 sort, 2 raster, 3 chain+Adam) is
+ * and each phase (0 projection + tile counts, 1 presort + entry expansion + tile
+ * sort + work order, 2 raster, 3 chain + Adam) is
  * bracketed by events on the launching stream.  gs_profile_read returns the
  * summed milliseconds and the number of timed launches per phase, then
  * clears them. */
