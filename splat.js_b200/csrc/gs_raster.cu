@@ -451,10 +451,15 @@ __global__ void __launch_bounds__(1024) k_work_order(const uint2* ranges, uint32
   __shared__ uint32_t s_off[33];
   if (threadIdx.x < 33) s_hist[threadIdx.x] = 0;
   __syncthreads();
-  for (uint32_t t = threadIdx.x; t < totalTiles; t += blockDim.x) {
-    const uint32_t len = ranges[t].y - ranges[t].x;
-    const uint32_t b = 32u - __clz(len);  // 0 for empty tiles
-    atomicAdd(&s_hist[32 - b], 1u);
+  // most tiles fall in a few buckets: one shared atomic per bucket per warp
+  // (whole warps step through the tiles; lanes past the end use bucket 64)
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t t0 = threadIdx.x - lane; t0 < totalTiles; t0 += blockDim.x) {
+    const uint32_t t = t0 + lane;
+    const bool valid = t < totalTiles;
+    const uint32_t b = valid ? (uint32_t)__clz(ranges[t].y - ranges[t].x) : 64u;  // 32: empty, 0: longest
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, b);
+    if (valid && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&s_hist[b], (uint32_t)__popc(peers));
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -462,10 +467,16 @@ __global__ void __launch_bounds__(1024) k_work_order(const uint2* ranges, uint32
     for (int b = 0; b < 33; ++b) { s_off[b] = acc; acc += s_hist[b]; }
   }
   __syncthreads();
-  for (uint32_t t = threadIdx.x; t < totalTiles; t += blockDim.x) {
-    const uint32_t len = ranges[t].y - ranges[t].x;
-    const uint32_t b = 32u - __clz(len);
-    order[atomicAdd(&s_off[32 - b], 1u)] = t;
+  for (uint32_t t0 = threadIdx.x - lane; t0 < totalTiles; t0 += blockDim.x) {
+    const uint32_t t = t0 + lane;
+    const bool valid = t < totalTiles;
+    const uint32_t b = valid ? (uint32_t)__clz(ranges[t].y - ranges[t].x) : 64u;
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, b);
+    const uint32_t lead = (uint32_t)(__ffs(peers) - 1);
+    uint32_t base = 0;
+    if (valid && lane == lead) base = atomicAdd(&s_off[b], (uint32_t)__popc(peers));
+    base = __shfl_sync(0xFFFFFFFFu, base, lead);
+    if (valid) order[base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = t;
   }
 }
 

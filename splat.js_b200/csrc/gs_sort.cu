@@ -148,7 +148,20 @@ __global__ void __launch_bounds__(256) k_radix_hist(RadixHistArgs a) {
   __syncthreads();
   const uint32_t N = *a.nItems;
   const KT* keys = static_cast<const KT*>(a.keys);
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+  // four keys per thread in flight, then their digits counted
+  const uint32_t stride = gridDim.x * blockDim.x;
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + 3 * stride < N; i += 4 * stride) {
+    const KT k0 = keys[i], k1 = keys[i + stride], k2 = keys[i + 2 * stride], k3 = keys[i + 3 * stride];
+    for (int p = 0; p < a.passes; ++p) {
+      const int sh = 8 * p;
+      atomicAdd(&h[p][(k0 >> sh) & 0xFF], 1u);
+      atomicAdd(&h[p][(k1 >> sh) & 0xFF], 1u);
+      atomicAdd(&h[p][(k2 >> sh) & 0xFF], 1u);
+      atomicAdd(&h[p][(k3 >> sh) & 0xFF], 1u);
+    }
+  }
+  for (; i < N; i += stride) {
     const KT k = keys[i];
     for (int p = 0; p < a.passes; ++p) atomicAdd(&h[p][(k >> (8 * p)) & 0xFF], 1u);
   }
