@@ -49,6 +49,7 @@ struct ExpandArgs {
   const uint2* rect;
   const RenderRec* recs;        // read when cull != 0 (the mean)
   const float4* cullRecs;       // read when cull != 0
+  uint4* itemRecs;              // V * n * 2: per presorted item (rect, mean, cull parameters, slot)
   const uint8_t* dropped;
   const uint32_t* viewDrops;
   float eCut, aMin;

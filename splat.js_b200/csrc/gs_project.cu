@@ -330,9 +330,29 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
   float4 cq = make_float4(__int_as_float(0x7F800000), 0.0f, 0.0f, 0.0f);
   s_run[threadIdx.x] = 0;
   if (valid) {
-    const uint32_t slot = a.sortedSlots[p];
-    const uint2 r = a.rect[slot];
-    if (KEYS) out = a.offsets[p];
+    // the item's rectangle, mean and cull parameters: gathered by slot in
+    // the count pass and written in presort order, so the key pass reads
+    // them coalesced
+    uint32_t slot;
+    uint2 r;
+    if (!KEYS) {
+      slot = a.sortedSlots[p];
+      r = a.rect[slot];
+      if (r.x != 0xFFFFFFFFu && a.cull) {
+        const float4 q0 = a.recs[slot].r0;
+        mx = q0.x; my = q0.y;
+        cq = a.cullRecs[slot];
+      }
+      a.itemRecs[2 * p] = make_uint4(r.x, r.y, __float_as_uint(mx), __float_as_uint(my));
+      a.itemRecs[2 * p + 1] = make_uint4(__float_as_uint(cq.x), __float_as_uint(cq.y), __float_as_uint(cq.z), slot);
+    } else {
+      const uint4 e0 = a.itemRecs[2 * p], e1 = a.itemRecs[2 * p + 1];
+      r = make_uint2(e0.x, e0.y);
+      mx = __uint_as_float(e0.z); my = __uint_as_float(e0.w);
+      cq = make_float4(__uint_as_float(e1.x), __uint_as_float(e1.y), __uint_as_float(e1.z), 0.0f);
+      slot = e1.w;
+      out = a.offsets[p];
+    }
     if (r.x != 0xFFFFFFFFu) {
       v = slot / a.n;
       i = slot - v * a.n;
@@ -340,11 +360,6 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
       x1 = r.y & 0xFFFFu;
       const uint32_t y1 = r.y >> 16;
       test = a.cull && !(x0 == x1 && y0 == y1);
-      if (test) {
-        const float4 q0 = a.recs[slot].r0;
-        mx = q0.x; my = q0.y;
-        cq = a.cullRecs[slot];
-      }
       if (a.viewDrops[v] == 0) {
         rr = y1 - y0 + 1;
       } else {

@@ -80,6 +80,7 @@ struct gs_trainer {
   uint32_t *counts = nullptr, *offsets = nullptr;
   float4* cullRecs = nullptr;
   float* viewGrad = nullptr;
+  uint4* itemRecs = nullptr;
   uint32_t* visList = nullptr;
   int32_t* gradP = nullptr;
   int32_t* diffGrid = nullptr;
@@ -386,6 +387,7 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   GS_AL(h->cullRecs, (size_t)B * cap);
   GS_AL(h->viewGrad, (size_t)B * cap * VIEWGRAD_STRIDE);
   GS_AL(h->visList, (size_t)B * cap);
+  GS_AL(h->itemRecs, (size_t)B * cap * 2);
   GS_AL(h->gradP, (size_t)B * cap * GP_STRIDE);
   // (tx+1)(ty+1) = tiles + tx + ty + 1 <= 3 * maxTiles + 1 for any view of at most maxTiles tiles
   GS_AL(h->diffGrid, (size_t)B * (3 * (size_t)h->maxTiles + 1));
@@ -633,6 +635,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   ea.rect = h->rect;
   ea.recs = h->recs;
   ea.cullRecs = h->cullRecs;
+  ea.itemRecs = h->itemRecs;
   ea.dropped = h->dropped;
   ea.viewDrops = h->viewDrops;
   ea.eCut = h->o.eCut;
