@@ -86,6 +86,43 @@ __device__ __forceinline__ float rcp_unit(float x) {
   return __fmaf_rn(e, y, y);
 }
 
+// ---- packed forms (two pixels per thread) ----------------------------------
+// sm_100 executes two FP32 operations per instruction (fma/mul/add.rn.f32x2),
+// each element rounded exactly as the scalar instruction; a scalar operand is
+// broadcast to both elements.  Each function below performs, element by
+// element, the same operation sequence as its scalar counterpart above, so
+// its results are bit-identical to two scalar calls.
+__device__ __forceinline__ float2 bc2(float s) { return make_float2(s, s); }
+
+__device__ __forceinline__ float2 gexp2(float2 x) {
+  const float RND = 12582912.0f;
+  const float2 t = __ffma2_rn(x, bc2(1.44269504088896341f), bc2(RND));
+  const float2 k = __fadd2_rn(t, bc2(-RND));  // t - RND: subtraction is addition of the negation
+  float2 r = __ffma2_rn(k, bc2(-0.693145751953125f), x);
+  r = __ffma2_rn(k, bc2(-1.42860676533018700e-6f), r);
+  float2 p = __ffma2_rn(bc2(1.98412698412698413e-4f), r, bc2(1.38888888888888889e-3f));
+  p = __ffma2_rn(p, r, bc2(8.33333333333333333e-3f));
+  p = __ffma2_rn(p, r, bc2(4.16666666666666667e-2f));
+  p = __ffma2_rn(p, r, bc2(1.66666666666666667e-1f));
+  p = __ffma2_rn(p, r, bc2(0.5f));
+  p = __ffma2_rn(p, r, bc2(1.0f));
+  p = __ffma2_rn(p, r, bc2(1.0f));
+  const float2 sb = make_float2(__uint_as_float((__float_as_uint(t.x) << 23) + 0x3F800000u),
+                                __uint_as_float((__float_as_uint(t.y) << 23) + 0x3F800000u));
+  return __fmul2_rn(p, sb);
+}
+
+__device__ __forceinline__ float2 rcp_unit2(float2 x) {
+  float2 y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y.x) : "f"(x.x));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y.y) : "f"(x.y));
+  const float2 nx = make_float2(-x.x, -x.y);
+  float2 e = __ffma2_rn(nx, y, bc2(1.0f));
+  y = __ffma2_rn(e, y, y);
+  e = __ffma2_rn(nx, y, bc2(1.0f));
+  return __ffma2_rn(e, y, y);
+}
+
 // log(x), x positive normal: x = m 2^e, m in [sqrt(1/2), sqrt(2)),
 // log m = 2 atanh((m-1)/(m+1)) by its odd series to degree 11.
 __device__ __forceinline__ float glog(float x) {

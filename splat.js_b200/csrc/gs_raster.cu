@@ -5,7 +5,9 @@
 // One CTA works on one TILE x TILE tile at a time (TILE = 8, 16 or 32; one
 // thread per pixel; each warp covers an 8x4 block of the tile).  Splat
 // records of the tile's sorted entries are staged in shared memory BATCH at
-// a time.
+// a time.  The fused train tile at TILE = 16 runs k_raster_px2 instead: two
+// pixels per thread on sm_100's packed FP32 instructions, each warp covering
+// an 8x8 block, with results identical to k_raster's.
 //
 // Forward: front-to-back compositing; the block leaves the tile when
 // __syncthreads_count (a block-wide ballot) finds every pixel saturated.  In
@@ -391,9 +393,353 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
   }
 }
 
+// Which 8x8 warp blocks of a 16x16 tile can the splat reach?  Bit w = warp w
+// (block row w / 2, column w % 2); the same band test as warp_block_mask on
+// 8-row bands.
+__device__ __forceinline__ uint32_t warp_block_mask8(const float4 cq, float mx, float my, int tx, int ty) {
+  if (!(cq.x < 3.0e38f)) return 0xFu;
+  uint32_t m = 0;
+#pragma unroll
+  for (int b = 0; b < 2; ++b) {
+    const float Y0 = ((float)(ty * 16 + 8 * b) + 0.5f) - my;
+    float xl, xr;
+    if (!bandInterval(cq, Y0, Y0 + 7.0f, xl, xr)) continue;
+#pragma unroll
+    for (int wb = 0; wb < 2; ++wb) {
+      const float bx0 = ((float)(tx * 16 + 8 * wb) + 0.5f) - mx;
+      if (bx0 + 7.0f >= xl && bx0 <= xr) m |= 1u << (b * 2 + wb);
+    }
+  }
+  return m;
+}
+
+// e = max(fma(fma(cA/2, dx, cB*dy), dx, ((cC/2)*dy)*dy), 0) for two pixels
+// that share dx; Bdy returns cB*dy.
+__device__ __forceinline__ float2 pairExponent2(const float4& r0, float hC, float dx, float2 dy, float2& Bdy) {
+  Bdy = __fmul2_rn(bc2(r0.w), dy);
+  const float2 u = __ffma2_rn(bc2(r0.z), bc2(dx), Bdy);
+  const float2 e = __ffma2_rn(u, bc2(dx), __fmul2_rn(__fmul2_rn(bc2(hC), dy), dy));
+  return make_float2(fmaxf(e.x, 0.0f), fmaxf(e.y, 0.0f));
+}
+
+#ifndef GS_RASTER_PX2_MIN_BLOCKS
+#define GS_RASTER_PX2_MIN_BLOCKS 7  // resident 128-thread blocks per SM the register allocation must allow
+#endif
+// Fused train tile (forward + loss + backward) on a 16x16 tile with two
+// pixels per thread: 128 threads, each warp covering an 8x8 block; lane l
+// holds pixels (l % 8, l / 8) and (l % 8, l / 8 + 4) of its block, which
+// share dx.  Every per-pixel operation runs on the pair with one packed
+// instruction (or twice, for comparisons, selects and conversions) and
+// performs the canonical sequence of k_raster on each pixel; the per-entry
+// work (record loads, votes, the ten warp reductions and the shared-memory
+// adds) is shared by 64 pixels instead of 32.  Results are bit-identical to
+// k_raster<16, BATCH, true, true, false>: the same entries reach every pixel
+// (an 8x8 block skips an entry only when neither of its 8x4 halves can use
+// it), and integer sums do not depend on how pixels are grouped.
+template <int BATCH>
+__global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(RasterArgs a) {
+  constexpr int NT = 128, NW = 4;
+  static_assert(BATCH % 32 == 0, "batches hold whole ballot words");
+  __shared__ RenderRec s_rec[BATCH];
+  __shared__ uint32_t s_id[BATCH];
+  __shared__ int32_t s_acc[BATCH * 10];
+  __shared__ uint32_t s_mask[NW * MASKW];
+  __shared__ uint32_t s_live[NW][BATCH / 32];
+  __shared__ uint32_t s_item;
+  __shared__ uint32_t s_redu[NW][5];
+  __shared__ uint32_t s_endmax[NW];
+  __shared__ __align__(16) int32_t s_stage[NW][12];
+
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int lx = (wid & 1) * 8 + (lane & 7);
+  const int ly = (wid >> 1) * 8 + (lane >> 3);  // pixel a; pixel b is 4 rows below
+  const float E_CUT = a.eCut, A_MIN = a.aMin;
+  uint32_t* wmask = s_mask + wid * MASKW;
+
+  for (int k = tid; k < BATCH * 10; k += NT) s_acc[k] = 0;
+
+  for (uint32_t iter = 0;; ++iter) {
+    if (tid == 0) s_item = a.workCounter ? atomicAdd(a.workCounter, 1u) : (iter == 0 ? blockIdx.x : 0xFFFFFFFFu);
+    __syncthreads();
+    const uint32_t item = s_item;
+    __syncthreads();
+    if (item >= a.totalTiles) break;
+    const uint32_t gt = a.workOrder ? a.workOrder[item] : item;
+    int v = 0;
+    while (v + 1 < a.V && a.cams[v + 1].tileBase <= gt) ++v;
+    const DevCam& c = a.cams[v];
+    const uint32_t t = gt - c.tileBase;
+    const int tx = (int)(t % (uint32_t)c.tilesX), ty = (int)(t / (uint32_t)c.tilesX);
+    const int x = tx * 16 + lx, ya = ty * 16 + ly, yb = ya + 4;
+    const bool inA = x < c.W && ya < c.H, inB = x < c.W && yb < c.H;
+    const float px = (float)x + 0.5f;
+    const float2 py = make_float2((float)ya + 0.5f, (float)yb + 0.5f);
+    const uint2 rg = a.ranges[gt];
+    const uint32_t s = rg.x, e = rg.y;
+    const size_t pixA = (size_t)c.pixBase + (size_t)ya * c.W + x;
+    const size_t pixB = pixA + (size_t)4 * c.W;
+    const RenderRec* recs = a.recs + (size_t)v * a.n;
+    const float4* cullRecs = a.cullRecs + (size_t)v * a.n;
+
+    // ---- forward ----
+    float2 T = bc2(1.0f);
+    float2 C0 = bc2(0.0f), C1 = bc2(0.0f), C2 = bc2(0.0f);
+    uint32_t cntA = e - s, cntB = e - s;
+    bool doneA = !inA, doneB = !inB;
+    for (int k = lane; k < MASKW; k += 32) wmask[k] = 0u;
+    __syncwarp();
+    for (uint32_t base = s; base < e; base += BATCH) {
+      if (__syncthreads_count(!(doneA && doneB)) == 0) break;
+      const uint32_t nb = min((uint32_t)BATCH, e - base);
+      for (uint32_t kb = 0; kb < (uint32_t)BATCH; kb += NT) {
+        const uint32_t k = kb + tid;
+        uint32_t m = 0;
+        if (k < nb) {
+          const uint32_t id = a.ids[base + k];
+          s_id[k] = id;
+          const RenderRec rec = recs[id];
+          s_rec[k] = rec;
+          m = warp_block_mask8(cullRecs[id], rec.r0.x, rec.r0.y, tx, ty);
+        }
+        const uint32_t word = (kb >> 5) + (uint32_t)wid;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+          const uint32_t bw = __ballot_sync(FULL, (m >> w) & 1u);
+          if (lane == 0 && word < (uint32_t)(BATCH / 32)) s_live[w][word] = bw;
+        }
+      }
+      __syncthreads();
+      if (!__all_sync(FULL, doneA && doneB)) {
+        const uint32_t rbase = base - s;
+        for (uint32_t jw = 0; jw < nb; jw += 32) {
+          uint32_t live = s_live[wid][jw >> 5];
+          uint32_t bits = 0;
+          while (live) {
+            const uint32_t jj = (uint32_t)__ffs(live) - 1u;
+            live &= live - 1u;
+            const RenderRec& rr = s_rec[jw + jj];
+            const float4 r0 = rr.r0;
+            const float4 r1 = rr.r1;
+            const float dx = px - r0.x;
+            const float2 dy = __fadd2_rn(py, bc2(-r0.y));
+            float2 Bdy;
+            const float2 ee = pairExponent2(r0, r1.x, dx, dy, Bdy);
+            const bool c1a = !doneA && ee.x <= E_CUT, c1b = !doneB && ee.y <= E_CUT;
+            if (__any_sync(FULL, c1a || c1b)) {
+              const float2 G = gexp2(make_float2(-fminf(ee.x, 80.0f), -fminf(ee.y, 80.0f)));
+              const float2 araw = __fmul2_rn(bc2(r1.y), G);
+              const float2 alpha = make_float2(fminf(0.99f, araw.x), fminf(0.99f, araw.y));
+              const bool c2a = c1a && alpha.x >= A_MIN, c2b = c1b && alpha.y >= A_MIN;
+              // a pixel that does not composite sees alpha 0: C and T stay exactly as they are
+              const float2 am = make_float2(c2a ? alpha.x : 0.0f, c2b ? alpha.y : 0.0f);
+              const float2 ta = __fmul2_rn(T, am);
+              C0 = __ffma2_rn(ta, bc2(r1.z), C0);
+              C1 = __ffma2_rn(ta, bc2(r1.w), C1);
+              C2 = __ffma2_rn(ta, bc2(rr.r2.x), C2);
+              T = __fmul2_rn(T, __fadd2_rn(bc2(1.0f), make_float2(-am.x, -am.y)));
+              if (c2a && T.x < 1e-4f) { doneA = true; cntA = rbase + jw + jj + 1; }
+              if (c2b && T.y < 1e-4f) { doneB = true; cntB = rbase + jw + jj + 1; }
+              bits |= (__ballot_sync(FULL, c2a || c2b) != 0u ? 1u : 0u) << jj;
+            }
+          }
+          const uint32_t w = (rbase + jw) >> 5;
+          if (lane == 0 && w < MASKW) wmask[w] = bits;
+          if (__all_sync(FULL, doneA && doneB)) break;
+        }
+      }
+      __syncthreads();
+    }
+    C0 = __fadd2_rn(C0, __fmul2_rn(T, bc2(c.bg[0])));
+    C1 = __fadd2_rn(C1, __fmul2_rn(T, bc2(c.bg[1])));
+    C2 = __fadd2_rn(C2, __fmul2_rn(T, bc2(c.bg[2])));
+    if (inA) {
+      if (a.outImg) a.outImg[pixA] = make_float4(C0.x, C1.x, C2.x, 1.0f - T.x);
+      if (a.finalT) a.finalT[pixA] = T.x;
+      if (a.endIdx) a.endIdx[pixA] = cntA;
+    }
+    if (inB) {
+      if (a.outImg) a.outImg[pixB] = make_float4(C0.y, C1.y, C2.y, 1.0f - T.y);
+      if (a.finalT) a.finalT[pixB] = T.y;
+      if (a.endIdx) a.endIdx[pixB] = cntB;
+    }
+
+    // ---- loss (shaders.js:589-618), per pixel ----
+    float2 gC0 = bc2(0.0f), gC1 = bc2(0.0f), gC2 = bc2(0.0f);
+    float2 g16_0 = bc2(0.0f), g16_1 = bc2(0.0f), g16_2 = bc2(0.0f);
+    uint32_t st0 = 0, st1 = 0, st2 = 0, cg6 = 0, cg7 = 0;
+    uint32_t myEndA = 0, myEndB = 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const bool in = h ? inB : inA;
+      if (!in) continue;
+      const int yy = h ? yb : ya;
+      const uint32_t pi = (uint32_t)(yy * c.W + x);
+      const uint32_t packed = a.targets[(size_t)c.offset + pi];
+      if ((packed >> 24) == 0u) continue;
+      const float Cx = h ? C0.y : C0.x, Cy = h ? C1.y : C1.x, Cz = h ? C2.y : C2.x;
+      const float t0 = (float)(packed & 0xFFu) / 255.0f;
+      const float t1 = (float)((packed >> 8) & 0xFFu) / 255.0f;
+      const float t2 = (float)((packed >> 16) & 0xFFu) / 255.0f;
+      st2 += 1u;
+      const float gain = c.gain;
+      const float er0 = (gain * Cx + c.bias) - t0;
+      const float er1 = (gain * Cy + c.bias) - t1;
+      const float er2 = (gain * Cz + c.bias) - t2;
+      st0 += u32sat((er0 * er0 + er1 * er1 + er2 * er2) * 16.0f + dither(pi));
+      const float D2 = 9.0000000000000003e-04f;  // f32(0.03 * 0.03), a WGSL const-expression
+      const float rt0 = sqrtf(er0 * er0 + D2), rt1 = sqrtf(er1 * er1 + D2), rt2 = sqrtf(er2 * er2 + D2);
+      const float eg0 = er0 / rt0, eg1 = er1 / rt1, eg2 = er2 / rt2;
+      const float q0 = gain * eg0, q1 = gain * eg1, q2 = gain * eg2;
+      const float lossv = (rt0 + rt1 + rt2) - 8.9999999999999997e-02f;  // f32(3 * 0.03)
+      st1 += u32sat(lossv * 32768.0f);
+      cg6 += (uint32_t)fixq((eg0 * Cx + eg1 * Cy + eg2 * Cz) * gain, FIXCAM);
+      cg7 += (uint32_t)fixq(eg0 + eg1 + eg2, FIXCAM);
+      if (h) {
+        gC0.y = q0; gC1.y = q1; gC2.y = q2;
+        g16_0.y = q0 * FIXED; g16_1.y = q1 * FIXED; g16_2.y = q2 * FIXED;
+        myEndB = cntB;
+      } else {
+        gC0.x = q0; gC1.x = q1; gC2.x = q2;
+        g16_0.x = q0 * FIXED; g16_1.x = q1 * FIXED; g16_2.x = q2 * FIXED;
+        myEndA = cntA;
+      }
+    }
+    // slots 7-9 stay within +-1e9 without clamping when |gC * 2^14| < 9e8
+    const bool pixFast = fabsf(g16_0.x) < 9.0e8f && fabsf(g16_1.x) < 9.0e8f && fabsf(g16_2.x) < 9.0e8f &&
+                         fabsf(g16_0.y) < 9.0e8f && fabsf(g16_1.y) < 9.0e8f && fabsf(g16_2.y) < 9.0e8f;
+    {
+      const uint32_t r0 = __reduce_add_sync(FULL, st0);
+      const uint32_t r1 = __reduce_add_sync(FULL, st1);
+      const uint32_t r2 = __reduce_add_sync(FULL, st2);
+      const uint32_t r3 = __reduce_add_sync(FULL, cg6);
+      const uint32_t r4 = __reduce_add_sync(FULL, cg7);
+      const uint32_t mx = __reduce_max_sync(FULL, max(myEndA, myEndB));
+      if (lane == 0) {
+        s_redu[wid][0] = r0; s_redu[wid][1] = r1; s_redu[wid][2] = r2;
+        s_redu[wid][3] = r3; s_redu[wid][4] = r4;
+        s_endmax[wid] = mx;
+      }
+    }
+    __syncthreads();
+    if (tid < 5) {
+      uint32_t sum = 0;
+      for (int w = 0; w < NW; ++w) sum += s_redu[w][tid];
+      if (sum) {
+        if (tid < 3) atomicAdd(&a.stats[tid], sum);
+        else atomicAdd(&a.gradCam[c.camIdx * 8u + 3u + (uint32_t)tid], (int32_t)sum);
+      }
+    }
+    uint32_t endMax = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) endMax = max(endMax, s_endmax[w]);
+
+    // ---- backward (shaders.js:632-700) ----
+    float2 S0 = __fmul2_rn(bc2(c.bg[0]), T), S1 = __fmul2_rn(bc2(c.bg[1]), T), S2 = __fmul2_rn(bc2(c.bg[2]), T);
+    float2 Ta = T;
+    int32_t* gradP = a.gradP + (size_t)v * a.n * GP_STRIDE;
+    for (uint32_t hi = endMax; hi > 0;) {
+      const uint32_t lo = hi > (uint32_t)BATCH ? hi - BATCH : 0u;
+      const uint32_t nb = hi - lo;
+      __syncthreads();
+      for (uint32_t k = tid; k < nb; k += NT) {
+        const uint32_t id = a.ids[s + lo + k];
+        s_id[k] = id;
+        s_rec[k] = recs[id];
+      }
+      __syncthreads();
+      for (int32_t w = (int32_t)((hi - 1) >> 5); w >= (int32_t)(lo >> 5); --w) {
+        const uint32_t wb = (uint32_t)w << 5;
+        uint32_t word = (uint32_t)w < (uint32_t)MASKW ? wmask[w] : FULL;
+        if (wb + 32u > hi) word &= FULL >> (wb + 32u - hi);
+        if (wb < lo) word &= FULL << (lo - wb);
+        while (word) {
+          const uint32_t bit = 31u - (uint32_t)__clz(word);
+          word &= ~(1u << bit);
+          const uint32_t j = wb + bit;
+          const RenderRec& rr = s_rec[j - lo];
+          const float4 r0 = rr.r0;
+          const float4 r1 = rr.r1;
+          const float4 r2 = rr.r2;
+          const float dx = px - r0.x;
+          const float2 dy = __fadd2_rn(py, bc2(-r0.y));
+          float2 Bdy;
+          const float2 ee = pairExponent2(r0, r1.x, dx, dy, Bdy);
+          const float2 G = gexp2(make_float2(-fminf(ee.x, 80.0f), -fminf(ee.y, 80.0f)));
+          const float2 araw = __fmul2_rn(bc2(r1.y), G);
+          const float2 alpha = make_float2(fminf(0.99f, araw.x), fminf(0.99f, araw.y));
+          const bool c2a = j < myEndA && ee.x <= E_CUT && alpha.x >= A_MIN;
+          const bool c2b = j < myEndB && ee.y <= E_CUT && alpha.y >= A_MIN;
+          if (!__any_sync(FULL, c2a || c2b)) continue;
+          const float2 inv = rcp_unit2(__fadd2_rn(bc2(1.0f), make_float2(-alpha.x, -alpha.y)));
+          const float2 Tb = __fmul2_rn(Ta, inv);
+          const float2 at = __fmul2_rn(alpha, Tb);
+          const float2 aT = make_float2(c2a ? at.x : 0.0f, c2b ? at.y : 0.0f);
+          const float2 g0 = __ffma2_rn(bc2(r1.z), Tb, __fmul2_rn(make_float2(-S0.x, -S0.y), inv));
+          const float2 g1 = __ffma2_rn(bc2(r1.w), Tb, __fmul2_rn(make_float2(-S1.x, -S1.y), inv));
+          const float2 g2 = __ffma2_rn(bc2(r2.x), Tb, __fmul2_rn(make_float2(-S2.x, -S2.y), inv));
+          const float2 gal = __ffma2_rn(gC2, g2, __ffma2_rn(gC1, g1, __fmul2_rn(gC0, g0)));
+          const float2 gal16r = __fmul2_rn(gal, bc2(FIXED));
+          const float2 gal16 = make_float2(c2a && !(araw.x > 0.99f) ? gal16r.x : 0.0f,
+                                           c2b && !(araw.y > 0.99f) ? gal16r.y : 0.0f);
+          const float2 ga16 = __fmul2_rn(gal16, araw);
+          const float cA = r0.z + r0.z, cC = r1.x + r1.x;
+          const float2 gq16 = __fmul2_rn(ga16, bc2(r2.z));
+          const float2 gqx16 = __fmul2_rn(gq16, bc2(dx));
+          float2 xs[10];
+          xs[0] = __fmul2_rn(ga16, __ffma2_rn(bc2(cA), bc2(dx), Bdy));
+          xs[1] = __fmul2_rn(ga16, __ffma2_rn(bc2(r0.w), bc2(dx), __fmul2_rn(bc2(cC), dy)));
+          xs[2] = __fmul2_rn(gqx16, bc2(dx));
+          xs[3] = __fmul2_rn(__fmul2_rn(gqx16, dy), bc2(2.0f));
+          xs[4] = __fmul2_rn(__fmul2_rn(gq16, dy), dy);
+          xs[5] = __fmul2_rn(__fmul2_rn(gal16, bc2(r2.y)), G);
+          xs[6] = __fmul2_rn(ga16, bc2(r2.w));
+          xs[7] = __fmul2_rn(g16_0, aT);
+          xs[8] = __fmul2_rn(g16_1, aT);
+          xs[9] = __fmul2_rn(g16_2, aT);
+          uint32_t rsum[10];
+          if (!__all_sync(FULL, fabsf(gal16.x) < 1.0e7f && fabsf(gal16.y) < 1.0e7f && pixFast)) {
+#pragma unroll
+            for (int k = 0; k < 10; ++k)
+              xs[k] = make_float2(fminf(fmaxf(xs[k].x, -1.0e9f), 1.0e9f), fminf(fmaxf(xs[k].y, -1.0e9f), 1.0e9f));
+          }
+#pragma unroll
+          for (int k = 0; k < 10; ++k)
+            rsum[k] = __reduce_add_sync(FULL, (uint32_t)__float2int_rz(xs[k].x) + (uint32_t)__float2int_rz(xs[k].y));
+          // a pixel that does not composite has aT = 0: S stays exactly as it is
+          S0 = __ffma2_rn(bc2(r1.z), aT, S0);
+          S1 = __ffma2_rn(bc2(r1.w), aT, S1);
+          S2 = __ffma2_rn(bc2(r2.x), aT, S2);
+          Ta = make_float2(c2a ? Tb.x : Ta.x, c2b ? Tb.y : Ta.y);
+          if (lane == 0) {
+            int4* st = reinterpret_cast<int4*>(s_stage[wid]);
+            st[0] = make_int4((int)rsum[0], (int)rsum[1], (int)rsum[2], (int)rsum[3]);
+            st[1] = make_int4((int)rsum[4], (int)rsum[5], (int)rsum[6], (int)rsum[7]);
+            reinterpret_cast<int2*>(s_stage[wid])[4] = make_int2((int)rsum[8], (int)rsum[9]);
+          }
+          __syncwarp();
+          if (lane < 10) atomicAdd(&s_acc[(j - lo) * 10 + (uint32_t)lane], s_stage[wid][lane]);
+          __syncwarp();
+        }
+      }
+      __syncthreads();
+      for (uint32_t k = tid; k < nb * 10; k += NT) {
+        const int32_t val = s_acc[k];
+        if (val) {
+          const uint32_t jl = k / 10, slot = k - jl * 10;
+          atomicAdd(&gradP[(size_t)s_id[jl] * GP_STRIDE + slot], val);
+          s_acc[k] = 0;
+        }
+      }
+      hi = lo;
+    }
+    __syncthreads();
+  }
+}
+
 template <int TILE, int BATCH, bool FWD, bool BWD, bool STORED>
 static void launch_one(const RasterArgs& a, unsigned grid, cudaStream_t s) {
-  k_raster<TILE, BATCH, FWD, BWD, STORED><<<grid, TILE * TILE, 0, s>>>(a);
+  if (TILE == 16 && FWD && BWD && !STORED) k_raster_px2<BATCH><<<grid, 128, 0, s>>>(a);
+  else k_raster<TILE, BATCH, FWD, BWD, STORED><<<grid, TILE * TILE, 0, s>>>(a);
 }
 
 template <int TILE, int BATCH>
@@ -426,21 +772,36 @@ void launch_raster(const RasterArgs& a, int mode, bool stored, int tile, int bat
   else launch_tile<16>(a, mode, stored, batchDepth, grid, s);
 }
 
+// The kernel launch_one runs for (TILE, depth, forward-only or fused train
+// tile, not stored) and its block size.
+template <int TILE, int BATCH>
+static const void* kernel_of_depth(bool fwdOnly, int& threads) {
+  threads = TILE * TILE;
+  if (fwdOnly) return (const void*)k_raster<TILE, BATCH, true, false, false>;
+  if (TILE == 16) {
+    threads = 128;
+    return (const void*)k_raster_px2<BATCH>;
+  }
+  return (const void*)k_raster<TILE, BATCH, true, true, false>;
+}
+
 template <int TILE>
-static const void* kernel_of(int batchDepth, int mode) {
+static const void* kernel_of(int batchDepth, int mode, int& threads) {
   const bool fwdOnly = mode == 1;
   switch (batchDepth) {
-    case 64: return fwdOnly ? (const void*)k_raster<TILE, 64, true, false, false> : (const void*)k_raster<TILE, 64, true, true, false>;
-    case 128: return fwdOnly ? (const void*)k_raster<TILE, 128, true, false, false> : (const void*)k_raster<TILE, 128, true, true, false>;
-    default: return fwdOnly ? (const void*)k_raster<TILE, 256, true, false, false> : (const void*)k_raster<TILE, 256, true, true, false>;
+    case 64: return kernel_of_depth<TILE, 64>(fwdOnly, threads);
+    case 128: return kernel_of_depth<TILE, 128>(fwdOnly, threads);
+    default: return kernel_of_depth<TILE, 256>(fwdOnly, threads);
   }
 }
 
 int raster_blocks_per_sm(int tile, int batchDepth, int mode) {
-  const void* f = tile == 8 ? kernel_of<8>(batchDepth, mode) : tile == 32 ? kernel_of<32>(batchDepth, mode)
-                                                                          : kernel_of<16>(batchDepth, mode);
+  int threads = 0;
+  const void* f = tile == 8 ? kernel_of<8>(batchDepth, mode, threads)
+                            : tile == 32 ? kernel_of<32>(batchDepth, mode, threads)
+                                         : kernel_of<16>(batchDepth, mode, threads);
   int perSm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, f, tile * tile, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, f, threads, 0);
   return perSm < 1 ? 1 : perSm;
 }
 
