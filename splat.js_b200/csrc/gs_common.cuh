@@ -195,6 +195,26 @@ __device__ __forceinline__ bool bandInterval(const float4 cq, float Y0, float Y1
   return true;
 }
 
+// bandInterval with the square root taken as rad2 * rsqrt(rad2) (a few ulp
+// instead of correctly rounded), for the rasteriser's warp-block masks only:
+// they need to be conservative, not reproducible, and the interval's 1e-5
+// relative and 4e-3 px absolute slack exceed that error by two orders of
+// magnitude.  The tile cull keeps bandInterval, which the oracle repeats.
+__device__ __forceinline__ bool bandIntervalMask(const float4 cq, float Y0, float Y1, float& xl, float& xr) {
+  const float p = cq.x, q = cq.y, kA = cq.z;
+  float d = Y0 > 0.0f ? Y0 : (Y1 < 0.0f ? -Y1 : 0.0f);
+  d = fmaxf(d - (1.0e-3f + 1.0e-6f * d), 0.0f);
+  const float rad2 = __fmaf_rn(-q, d * d, p) + 1.0e-5f * p;
+  if (!(rad2 >= 0.0f)) return false;
+  const float r = (rad2 > 0.0f ? rad2 * rsqrtf(rad2) : 0.0f) * 1.00001f;
+  const float c0 = kA * Y0, c1 = kA * Y1;
+  const float cl = fminf(c0, c1), ch = fmaxf(c0, c1);
+  const float sl = 4.0e-3f * (1.0f + fabsf(kA)) + 1.0e-5f * (fabsf(cl) + fabsf(ch) + r);
+  xl = (cl - r) - sl;
+  xr = (ch + r) + sl;
+  return true;
+}
+
 // Tile cull: can any pixel centre of tile (tx, ty) (clipped to the W x H
 // image) be reachable?  A (splat, tile) entry that fails cannot composite
 // into any pixel of the tile, so dropping it changes no image, loss or

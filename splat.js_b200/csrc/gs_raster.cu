@@ -403,7 +403,7 @@ __device__ __forceinline__ uint32_t warp_block_mask8(const float4 cq, float mx, 
   for (int b = 0; b < 2; ++b) {
     const float Y0 = ((float)(ty * 16 + 8 * b) + 0.5f) - my;
     float xl, xr;
-    if (!bandInterval(cq, Y0, Y0 + 7.0f, xl, xr)) continue;
+    if (!bandIntervalMask(cq, Y0, Y0 + 7.0f, xl, xr)) continue;
 #pragma unroll
     for (int wb = 0; wb < 2; ++wb) {
       const float bx0 = ((float)(tx * 16 + 8 * wb) + 0.5f) - mx;
@@ -488,6 +488,11 @@ __global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(Ra
     bool doneA = !inA, doneB = !inB;
     for (int k = lane; k < MASKW; k += 32) wmask[k] = 0u;
     __syncwarp();
+    // each batch's entry values are loaded while the previous batch is
+    // processed (two per thread), so staging starts with the record gathers
+    static_assert(BATCH <= 2 * NT, "two prefetched values per thread");
+    uint32_t pf0 = s + (uint32_t)tid < e ? a.ids[s + tid] : 0u;
+    uint32_t pf1 = BATCH > NT && s + NT + (uint32_t)tid < e ? a.ids[s + NT + tid] : 0u;
     for (uint32_t base = s; base < e; base += BATCH) {
       if (__syncthreads_count(!(doneA && doneB)) == 0) break;
       const uint32_t nb = min((uint32_t)BATCH, e - base);
@@ -495,7 +500,7 @@ __global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(Ra
         const uint32_t k = kb + tid;
         uint32_t m = 0;
         if (k < nb) {
-          const uint32_t id = a.ids[base + k];
+          const uint32_t id = kb == 0 ? pf0 : pf1;
           s_id[k] = id;
           const RenderRec rec = recs[id];
           s_rec[k] = rec;
@@ -509,6 +514,11 @@ __global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(Ra
         }
       }
       __syncthreads();
+      {
+        const uint32_t nx = base + BATCH;
+        pf0 = nx + (uint32_t)tid < e ? a.ids[nx + tid] : 0u;
+        pf1 = BATCH > NT && nx + NT + (uint32_t)tid < e ? a.ids[nx + NT + tid] : 0u;
+      }
       if (!__all_sync(FULL, doneA && doneB)) {
         const uint32_t rbase = base - s;
         for (uint32_t jw = 0; jw < nb; jw += 32) {
