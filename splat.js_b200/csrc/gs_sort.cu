@@ -346,22 +346,44 @@ __global__ void __launch_bounds__(RS_THREADS, GS_SORT_MIN_BLOCKS) k_onesweep(One
           *reinterpret_cast<unsigned long long*>(a.status + (size_t)tile * 256 + d));
       uint32_t excl = 0;
       if (tile != 0) {
+        // LB predecessors' words are loaded at once and summed nearest first
+        // up to the first inclusive one; a word not yet published ends the
+        // round there, and the next round starts from it
+        constexpr int LB = 4;
         int64_t t = (int64_t)tile - 1;
         uint32_t spins = 0;
         while (t >= 0) {
-          cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> pr(
-              *reinterpret_cast<unsigned long long*>(a.status + (size_t)t * 256 + d));
-          const unsigned long long sw = pr.load(cuda::memory_order_relaxed);
-          const uint32_t stag = (uint32_t)(sw >> 32);
-          const uint32_t flag = (uint32_t)(sw >> 30) & 3u;
-          if (stag != tag || flag == 0) {
+          unsigned long long w[LB];
+#pragma unroll
+          for (int k = 0; k < LB; ++k) {
+            w[k] = 0ull;
+            if (t - k >= 0) {
+              cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> pr(
+                  *reinterpret_cast<unsigned long long*>(a.status + (size_t)(t - k) * 256 + d));
+              w[k] = pr.load(cuda::memory_order_relaxed);
+            }
+          }
+          int used = 0, state = 0;  // state: 0 keep going, 1 inclusive word found, 2 a word not ready
+#pragma unroll
+          for (int k = 0; k < LB; ++k) {
+            if (state == 0 && t - k >= 0) {
+              const uint32_t stag = (uint32_t)(w[k] >> 32);
+              const uint32_t flag = (uint32_t)(w[k] >> 30) & 3u;
+              if (stag != tag || flag == 0) {
+                state = 2;
+              } else {
+                excl += (uint32_t)(w[k] & 0x3FFFFFFFull);
+                ++used;
+                if (flag == FLAG_INC) state = 1;
+              }
+            }
+          }
+          if (state == 1) break;
+          t -= used;
+          if (state == 2) {
             if (++spins > a.spinLimit) { atomicOr(a.statusWord, ST_LOOKBACK_TIMEOUT); break; }
             __nanosleep(32);
-            continue;
           }
-          excl += (uint32_t)(sw & 0x3FFFFFFFull);
-          if (flag == FLAG_INC) break;
-          --t;
         }
         my.store(((unsigned long long)tag << 32) | ((unsigned long long)FLAG_INC << 30) | (excl + run),
                  cuda::memory_order_relaxed);
