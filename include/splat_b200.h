@@ -212,6 +212,29 @@ GS_API int gs_probe_fp32_peak(int32_t device, double* tflops);
  * *mismatches must be 0 (*firstBits: the first failing x's bits). */
 GS_API int gs_debug_check_rcp(int32_t device, uint64_t* mismatches, uint32_t* firstBits);
 
+/* ---- target ingestion ----
+ * A training frame for gs_undistort_frames: tw x th pixels, 3 floats each
+ * (rgb, modified in place), fw = the width the camera model's focal length
+ * fFeat refers to (the frame's feature-extraction width). */
+typedef struct gs_frame {
+  uint32_t tw, th;
+  double fw;
+  float* rgb;
+} gs_frame;
+/* undistortFrames(frames, recon) (session.js:44-80): resamples every frame
+ * in place through the radial model D = 1 + k1 r^2 + k2 r^4 (bilinear, in
+ * double precision, float32 results identical to the JavaScript's); a pixel
+ * whose source falls outside the frame becomes -1 in all three channels,
+ * which setup packs as an invalid target.  |k1| and |k2| both below 0.01
+ * change nothing (*resampled = 0), as in the reference.  Runs on `device`;
+ * allocates and frees its own scratch. */
+GS_API int gs_undistort_frames(int32_t device, gs_frame* frames, uint32_t nframes, double k1, double k2,
+                               double fFeat, int32_t* resampled);
+/* The packed RGBA8 targets gs_setup built (trainer.js:115-139), pixels
+ * [0, count) in camera-offset order (no reference counterpart: parity
+ * introspection). */
+GS_API int gs_debug_targets(gs_trainer* h, uint32_t* out, uint64_t count);
+
 /* ---- allocation-free entry sort (no counterpart in the reference) ----
  * For callers that cannot call cudaMalloc: code whose device memory is owned
  * by another runtime's pool (a host application or binding that forbids

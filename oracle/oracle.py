@@ -306,3 +306,57 @@ def ply_export(params, n, sh=None, shK=0, bake=False, f=0.0, cam_positions=()):
     q[small] = [1.0, 0.0, 0.0, 0.0]
     rec[:, q0 + 4:q0 + 8] = q
     return header.encode() + rec.astype('<f4').tobytes()
+
+
+def undistort_frames(frames, recon):
+    """session.js:44-80 (undistortFrames) restated in numpy float64 with the
+    JavaScript's operation order and float32 stores; returns (resampled,
+    list of new rgb arrays).  Out-of-frame pixels get -1 in every channel."""
+    k1, k2 = float(recon["k1"]), float(recon["k2"])
+    if abs(k1) < 0.01 and abs(k2) < 0.01:
+        return False, [np.asarray(im["rgb"], np.float32) for im in frames]
+    out = []
+    for im in frames:
+        tw, th = int(im["tw"]), int(im["th"])
+        f = float(recon["fFeat"]) * (tw / float(im["fw"]))        # session.js:50
+        cx, cy = tw / 2, th / 2
+        src = np.asarray(im["rgb"], np.float32).reshape(th, tw, 3).astype(np.float64)
+        x = np.arange(tw, dtype=np.float64)[None, :]
+        y = np.arange(th, dtype=np.float64)[:, None]
+        xp = (x + 0.5 - cx) / f                                   # :55-59, left to right
+        yp = (y + 0.5 - cy) / f
+        r2 = xp * xp + yp * yp
+        D = 1 + k1 * r2 + k2 * r2 * r2
+        rx = f * xp * D + cx - 0.5
+        ry = f * yp * D + cy - 0.5
+        rx, ry = np.broadcast_to(rx, (th, tw)), np.broadcast_to(ry, (th, tw))
+        outside = (rx < 0) | (ry < 0) | (rx > tw - 1.001) | (ry > th - 1.001)   # :61
+        rxi = np.where(outside, 0.0, rx)
+        ryi = np.where(outside, 0.0, ry)
+        x0 = rxi.astype(np.int64)                                 # rx | 0
+        y0 = ryi.astype(np.int64)
+        fx, fy = rxi - x0, ryi - y0
+        x1, y1 = np.minimum(x0 + 1, tw - 1), np.minimum(y0 + 1, th - 1)
+        s00, s01 = src[y0, x0], src[y0, x1]
+        s10, s11 = src[y1, x0], src[y1, x1]
+        fx3, fy3 = fx[..., None], fy[..., None]
+        v = s00 * (1 - fx3) * (1 - fy3) + s01 * fx3 * (1 - fy3) + s10 * (1 - fx3) * fy3 + s11 * fx3 * fy3   # :71-74
+        dst = v.astype(np.float32)
+        dst[outside] = -1.0
+        out.append(dst.reshape(-1))
+    return True, out
+
+
+def pack_rgba8(rgb):
+    """GSTrainer.setup's target packing for one image (trainer.js:127-136):
+    alpha 255 with min(255, round(255 v)) per channel (low byte), or the
+    whole word 0 where red < 0."""
+    a = np.asarray(rgb, np.float32).reshape(-1, 3)
+
+    def r255(v):
+        x = np.floor(v.astype(np.float64) * 255.0 + 0.5)
+        return (np.minimum(x, 255.0).astype(np.int64) & 0xFF).astype(np.uint32)
+
+    packed = (np.uint32(255) << np.uint32(24)) | (r255(a[:, 2]) << np.uint32(16)) | \
+        (r255(a[:, 1]) << np.uint32(8)) | r255(a[:, 0])
+    return np.where(a[:, 0] < 0, np.uint32(0), packed).astype(np.uint32)

@@ -195,6 +195,9 @@ uint32_t scan_partials_needed(uint64_t N);
 void launch_exclusive_scan(const uint32_t* in, uint64_t N, uint32_t* out, uint32_t* partials, uint32_t* total,
                            cudaStream_t s);
 int onesweep_grid(int device);
+// RGBA8 packing of one camera's float RGB target (host memory) into out,
+// staged through scratch (3 floats per pixel) on stream s.
+int pack_targets_device(const float* rgbHost, uint64_t np, float* scratch, uint32_t* out, cudaStream_t s);
 int export_ply_records(const float* params, const float* sh, uint32_t n, uint32_t K, int bake, double f,
                        const double* camPosHost, uint32_t ncams, float* outHost, cudaStream_t s);
 int debug_lookback_timeout(int device, uint32_t spinLimit, uint32_t* statusOut, double* msOut);

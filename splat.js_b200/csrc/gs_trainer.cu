@@ -336,21 +336,11 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   }
   if (total > 0xFFFFFFFFull) return fail(h, GS_E_LIMIT, "setup: training targets exceed 2^32 pixels");
   h->totalPix = total;
-  std::vector<uint32_t> packed(std::max<uint64_t>(total, 4), 0u);
-  auto r255 = [](float v) -> uint32_t {
-    double x = std::floor((double)v * 255.0 + 0.5);
-    if (x > 255.0) x = 255.0;
-    return (uint32_t)(int64_t)x & 0xFFu;
-  };
+  uint64_t maxImgPix = 0;
   for (uint32_t c = 0; c < ncams; ++c) {
     const gs_image& im = images[cams[c].imgIdx];
-    const uint64_t np = (uint64_t)im.tw * im.th;
-    uint32_t* dst = packed.data() + h->camOffset[c];
-    for (uint64_t p = 0; p < np; ++p) {
-      const float r = im.rgb[p * 3];
-      if (r < 0.0f) { dst[p] = 0u; continue; }
-      dst[p] = (255u << 24) | (r255(im.rgb[p * 3 + 2]) << 16) | (r255(im.rgb[p * 3 + 1]) << 8) | r255(r);
-    }
+    if (!im.rgb && im.tw && im.th) return fail(h, GS_E_INVALID, "setup: image without pixels");
+    maxImgPix = std::max<uint64_t>(maxImgPix, (uint64_t)im.tw * im.th);
   }
   // view limits
   h->maxPix = maxViewW * maxViewH;
@@ -431,7 +421,24 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   GS_CK(cudaMemsetAsync(h->gradP, 0, (size_t)B * cap * GP_STRIDE * 4, s));
   GS_CK(cudaMemsetAsync(h->small, 0, 4096 * 4, s));
   GS_CK(cudaMemsetAsync(h->lbStatus, 0, (size_t)(std::max<uint64_t>(h->capacity, (uint64_t)B * cap) / SORT_BLOCK_ENTRIES + 2) * 256 * 8, s));
-  GS_CK(cudaMemcpyAsync(h->targets, packed.data(), std::max<uint64_t>(total, 4) * 4, cudaMemcpyHostToDevice, s));
+  // targets packed on the device, one camera at a time through a scratch
+  // buffer of the largest image
+  {
+    float* scratch = nullptr;
+    if (maxImgPix && cudaMalloc(&scratch, maxImgPix * 12) != cudaSuccess) {
+      free_all(h);
+      return fail(h, GS_E_NOMEM, "setup: target staging buffer");
+    }
+    GS_CK(cudaMemsetAsync(h->targets, 0, std::max<uint64_t>(total, 4) * 4, s));
+    int prc = 0;
+    for (uint32_t c = 0; c < ncams && prc == 0; ++c) {
+      const gs_image& im = images[cams[c].imgIdx];
+      prc = pack_targets_device(im.rgb, (uint64_t)im.tw * im.th, scratch, h->targets + h->camOffset[c], s);
+    }
+    const cudaError_t se = cudaStreamSynchronize(s);
+    cudaFree(scratch);
+    if (prc != 0 || se != cudaSuccess) return fail(h, GS_E_CUDA, "setup: target packing");
+  }
   GS_CK(cudaMemsetAsync(h->stats, 0, 16, s));
   GS_CK(cudaMemsetAsync(h->gradCam, 0, (size_t)(ncams + 1) * 32, s));
   GS_CK(cudaStreamSynchronize(s));
@@ -1106,6 +1113,14 @@ int gs_debug_binning(gs_trainer* h, uint32_t view, uint32_t* tileCnt, uint32_t* 
     GS_CK(cudaMemcpyAsync(ids, h->vals[h->lastPasses & 1], k * 4, cudaMemcpyDeviceToHost, h->stream));
     GS_CK(cudaStreamSynchronize(h->stream));
   }
+  return GS_OK;
+}
+
+int gs_debug_targets(gs_trainer* h, uint32_t* out, uint64_t count) {
+  if (!h || !h->ready || !out || count > h->totalPix) return GS_E_INVALID;
+  cudaSetDevice(h->device);
+  if (count) GS_CK(cudaMemcpyAsync(out, h->targets, count * 4, cudaMemcpyDeviceToHost, h->stream));
+  GS_CK(cudaStreamSynchronize(h->stream));
   return GS_OK;
 }
 

@@ -38,6 +38,10 @@ class GsImage(C.Structure):
     _fields_ = [("tw", C.c_uint32), ("th", C.c_uint32), ("rgb", C.POINTER(C.c_float))]
 
 
+class GsFrame(C.Structure):
+    _fields_ = [("tw", C.c_uint32), ("th", C.c_uint32), ("fw", C.c_double), ("rgb", C.POINTER(C.c_float))]
+
+
 GS_E_LIMIT = -5
 STATIC_SORT_MAX = 1 << 20  # GS_STATIC_SORT_MAX of include/splat_b200.h
 
@@ -114,6 +118,9 @@ def lib():
         "gs_debug_pixels": (C.c_int, [H, C.c_uint32, f32p, f32p, u32p]),
         "gs_debug_lookback_timeout": (C.c_int, [C.c_int32, C.c_uint32, u32p, P(C.c_double)]),
         "gs_debug_gradp": (C.c_int, [H, C.c_uint32, i32p, C.c_int32]),
+        "gs_undistort_frames": (C.c_int, [C.c_int32, P(GsFrame), C.c_uint32, C.c_double, C.c_double, C.c_double,
+                                          i32p]),
+        "gs_debug_targets": (C.c_int, [H, u32p, C.c_uint64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
