@@ -436,6 +436,42 @@ def test_needles_and_discs_bitexact(tile):
     check_view_against_oracle(t, oracle_opts(opts), oracle_cam(metas[0], 0, 1, 2), params, sh, targets, n)
 
 
+def deep_tile_scene(n, seed=0, W=64, H=64):
+    """n small, faint splats crowded over one 16x16 tile: its list holds far
+    more than 4096 entries (past the rasteriser's ballot-bit capacity and
+    over many shared-memory batches) while no pixel saturates."""
+    rng = np.random.default_rng(seed)
+    P = np.zeros((n, 16), np.float32)
+    # tile (2, 2) of a 64x64 view at f = 64, z = 3: world x, y in [0, 0.75)
+    P[:, 0] = rng.uniform(0.02, 0.73, n)
+    P[:, 1] = rng.uniform(0.02, 0.73, n)
+    P[:, 2] = rng.uniform(-0.2, 0.2, n)
+    P[:, 3:6] = rng.uniform(-4.2, -3.4, (n, 3))
+    q = rng.normal(size=(n, 4))
+    P[:, 6:10] = q / np.linalg.norm(q, axis=1, keepdims=True)
+    P[:, 10:13] = rng.normal(0, 1.0, (n, 3))
+    P[:, 13] = rng.uniform(-5.0, -3.8, n)
+    R, t = scene.look_at_pose([0.0, 0.0, -3.0], [0.0, 0.0, 0.0])
+    cam = dict(R=R, t=t, f=64.0, cx=W / 2, cy=H / 2, w=W, h=H)
+    return P.reshape(-1), cam
+
+
+@pytest.mark.parametrize("depth", [64, 256])
+def test_deep_tile_bitexact(depth):
+    """A tile list past 4096 entries: the backward walks those entries without
+    ballot bits; images, lists and gradients must still match the oracle."""
+    n = 9000
+    params, cam = deep_tile_scene(n)
+    sh = np.zeros(n * 3 * 8, np.float32)
+    opts = dict(shDeg=2, batchDepth=depth)
+    t, targets, metas = make(params, sh, [cam], [scene.uniform_target(64, 64, seed=5)], opts, radius=1.0)
+    gpu_raster(t, [0], 3)
+    g, r, proj, b = check_view_against_oracle(t, oracle_opts(opts), oracle_cam(metas[0], 0, 1, 2), params, sh,
+                                              targets, n)
+    assert np.diff(b["start"]).max() > 4096      # a list past the bit capacity
+    assert np.asarray(r["end"]).max() > 4096     # and pixels that composite past it
+
+
 def test_lookback_timeout_is_reported_and_device_stays_usable():
     """A sort pass whose look-back can never complete gives up after a bounded
     number of spins, sets the timeout bit, and leaves the device usable."""
