@@ -50,6 +50,7 @@ struct ExpandArgs {
   const RenderRec* recs;        // read when cull != 0 (the mean)
   const float4* cullRecs;       // read when cull != 0
   uint4* itemRecs;              // V * n * 2: per presorted item (rect, mean, cull parameters, slot)
+  const uint32_t* presortHist;  // the presort's digit histograms (4 x 256): culled items = [3 * 256 + 255]
   const uint8_t* dropped;
   const uint32_t* viewDrops;
   float eCut, aMin;

@@ -319,11 +319,19 @@ template <bool KEYS>
 __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
   __shared__ uint32_t s_run[256];  // entries of each item so far
   const uint64_t items = (uint64_t)a.n * a.V;
+  // culled items carry the all-ones key, the only key whose top byte is 0xFF
+  // (depth bits of a positive float are below 0x7F800000): the presort puts
+  // them last and its top-digit histogram counts them
+  const uint64_t live = items - a.presortHist[3 * 256 + 255];
   const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if ((uint64_t)blockIdx.x * blockDim.x >= live) {  // the whole block is culled items (uniform)
+    if (!KEYS && p < items) a.counts[p] = 0u;
+    return;
+  }
   const int lane = threadIdx.x & 31;
   const int wbase = threadIdx.x & ~31;
   const uint32_t FULL = 0xFFFFFFFFu;
-  const bool valid = p < items;
+  const bool valid = p < live;
   uint32_t v = 0, i = 0, x0 = 0, x1 = 0, y0 = 0, rr = 0, out = 0;
   bool test = false;
   float mx = 0.0f, my = 0.0f;
@@ -477,7 +485,7 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
     if (inRange && lane == lead) s_run[wbase + lo] = prior + gsum;
     __syncwarp();
   }
-  if (!KEYS && valid) a.counts[p] = s_run[threadIdx.x];
+  if (!KEYS && p < items) a.counts[p] = valid ? s_run[threadIdx.x] : 0u;
 }
 
 // Per-tile ranges from the sorted entry keys (culled lists): tile gt spans

@@ -643,6 +643,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   ea.recs = h->recs;
   ea.cullRecs = h->cullRecs;
   ea.itemRecs = h->itemRecs;
+  ea.presortHist = hist;
   ea.dropped = h->dropped;
   ea.viewDrops = h->viewDrops;
   ea.eCut = h->o.eCut;
