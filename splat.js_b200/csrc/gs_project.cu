@@ -30,7 +30,7 @@ namespace gs {
 // One thread per splat, looping over the batch's views: parameters and SH
 // coefficients are read once per step.
 template <int DEG>
-__global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
+__global__ void __launch_bounds__(256, 4) k_project(ProjectArgs a) {  // 4 blocks/SM: 64 registers
   constexpr int K = DEG > 0 ? (DEG + 1) * (DEG + 1) - 1 : 0;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   // the batch's cameras in shared memory (read once per block); each thread
