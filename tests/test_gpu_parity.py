@@ -472,6 +472,24 @@ def test_deep_tile_bitexact(depth):
     assert np.asarray(r["end"]).max() > 4096     # and pixels that composite past it
 
 
+def test_full_size_views_bitexact():
+    """The benchmark's own workload: 1M-splat surface scene, two 1920x1080
+    ring views batched in one raster pass -- every record, per-tile list,
+    pixel and fixed-point gradient against the oracle."""
+    n = 1_000_000
+    params, sh = scene.surface_scene(n, seed=0, sh_deg=2, log_scale=(-5.0, 0.7))
+    ring = scene.ring_cameras(24, 4.0, 0.5, 1920, 1080)
+    cams = [ring[0], ring[7]]
+    rgbs = [scene.uniform_target(1920, 1080, seed=7 + k) for k in range(2)]
+    # the entry budget of trainer.js:48-49 at maxSplats = 1M: max(12M, 24 n)
+    opts = dict(shDeg=2, maxSplats=n, batchDepth=256, entriesCap=24 * n)
+    t, targets, metas = make(params, sh, cams, rgbs, opts, radius=4.0)
+    gpu_raster(t, [0, 1], 3)
+    for v in range(2):
+        check_view_against_oracle(t, oracle_opts(opts), oracle_cam(metas[v], v, 2, 2), params, sh, targets, n,
+                                  view=v)
+
+
 def test_lookback_timeout_is_reported_and_device_stays_usable():
     """A sort pass whose look-back can never complete gives up after a bounded
     number of spins, sets the timeout bit, and leaves the device usable."""
