@@ -475,7 +475,8 @@ def test_deep_tile_bitexact(depth):
 def test_full_size_views_bitexact():
     """The benchmark's own workload: 1M-splat surface scene, two 1920x1080
     ring views batched in one raster pass -- every record, per-tile list,
-    pixel and fixed-point gradient against the oracle."""
+    pixel and fixed-point gradient against the oracle -- then one optimiser
+    step over both views: every parameter and SH coefficient after Adam."""
     n = 1_000_000
     params, sh = scene.surface_scene(n, seed=0, sh_deg=2, log_scale=(-5.0, 0.7))
     ring = scene.ring_cameras(24, 4.0, 0.5, 1920, 1080)
@@ -484,10 +485,22 @@ def test_full_size_views_bitexact():
     # the entry budget of trainer.js:48-49 at maxSplats = 1M: max(12M, 24 n)
     opts = dict(shDeg=2, maxSplats=n, batchDepth=256, entriesCap=24 * n)
     t, targets, metas = make(params, sh, cams, rgbs, opts, radius=4.0)
+    t.iter = 2000
     gpu_raster(t, [0, 1], 3)
+    o = oracle_opts(opts)
     for v in range(2):
-        check_view_against_oracle(t, oracle_opts(opts), oracle_cam(metas[v], v, 2, 2), params, sh, targets, n,
-                                  view=v)
+        check_view_against_oracle(t, o, oracle_cam(metas[v], v, 2, 2), params, sh, targets, n, view=v)
+    # and one optimiser step over both views: parameters and SH after Adam
+    K = 8
+    m, vv = np.zeros(n * 16, np.float32), np.zeros(n * 16, np.float32)
+    sm, sv = np.zeros(n * 3 * K, np.float32), np.zeros(n * 3 * K, np.float32)
+    p, s = params.copy(), sh.copy()
+    t.stepBatch([0, 1])
+    O.step(o, [oracle_cam(metas[v], v, 2, 2) for v in range(2)], oracle_adam(t, 2001, 4.0), p, s, targets, m, vv,
+           sm, sv, n)
+    g = t.readGaussians()
+    assert_bits(g["data"], p, "params after a full-size batched step")
+    assert_bits(g["sh"], s, "SH after a full-size batched step")
 
 
 def test_lookback_timeout_is_reported_and_device_stays_usable():
