@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(128, GS_CHAIN_MIN_BLOCKS) k_chain_view(ChainAr
   // global memory around every store); every thread issues its own loads
   // before the barrier that publishes it
   __shared__ DevCam s_cam;
-  if (threadIdx.x == 0) s_cam = a.cams[v];
+  copy_cams(&s_cam, a.cams + v, 1);
   const size_t slot = (size_t)v * a.n + i;
   int4 q0 = make_int4(0, 0, 0, 0), q1 = q0, q2 = q0;
   float P[16];

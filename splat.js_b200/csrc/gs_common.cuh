@@ -43,6 +43,17 @@ struct DevCam {
   uint32_t pixBase;    // first pixel of this view in the batch's pixel buffers
 };
 
+// Copy n camera records to shared memory with every thread of the block
+// taking 4-byte words, so the copy costs one load latency, not a chain of
+// them in one thread (the caller's barrier publishes it).
+static_assert(sizeof(DevCam) % 4 == 0, "camera records copy as words");
+__device__ __forceinline__ void copy_cams(DevCam* dst, const DevCam* src, int n) {
+  const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+  uint32_t* d = reinterpret_cast<uint32_t*>(dst);
+  const int words = n * (int)(sizeof(DevCam) / 4);
+  for (int k = threadIdx.x; k < words; k += blockDim.x) d[k] = s[k];
+}
+
 // Per-(view, splat) record read by the rasteriser: 3 x float4 = 48 B.
 //   r0 = (mx, my, cA/2, cB)  r1 = (cC/2, w = opa*comp, r, g)  r2 = (b, opa, -cnorm/2, 1 - opa)
 struct __align__(16) RenderRec {

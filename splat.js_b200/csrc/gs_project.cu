@@ -36,7 +36,7 @@ __global__ void __launch_bounds__(256, 4) k_project(ProjectArgs a) {  // 4 block
   // the batch's cameras in shared memory (read once per block); each thread
   // issues its parameter loads before the barrier that publishes them
   __shared__ DevCam s_cams[MAX_VIEWS];
-  for (int k = threadIdx.x; k < a.V; k += blockDim.x) s_cams[k] = a.cams[k];
+  copy_cams(s_cams, a.cams, a.V);
   float P[16];
   if (i < a.n) {
     const float4* P4 = reinterpret_cast<const float4*>(a.params + (size_t)i * STRIDE);
