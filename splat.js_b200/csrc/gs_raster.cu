@@ -31,8 +31,9 @@
 // no divergent branch needs a reconvergence scaffold in the hot loops.
 // The per-pair arithmetic is the canonical FP32 sequence the CPU
 // restatement performs.  The 2^14 fixed-point scale is folded into upstream
-// factors (galpha, gC): scaling by a power of two is exact, so every
-// truncated integer equals the one the unfolded sequence produces.  The
+// factors (gC, hence galpha, which is accumulated from the scaled gC):
+// scaling by a power of two is exact, so every truncated integer equals the
+// one the unfolded sequence produces.  The
 // +-1e9 clamp is skipped when a warp's scaled galpha is below 1e7: the
 // conic normaliser bounds every slot by 80 |galpha * 2^14| (slots 7-9 by
 // |gC * 2^14|), so the clamp cannot change a value then.
@@ -228,7 +229,6 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
       // ---- loss (shaders.js:589-618) ----
       bool lossOk = false;
       float g16_0 = 0.0f, g16_1 = 0.0f, g16_2 = 0.0f;  // gC * 2^14
-      float gC0 = 0.0f, gC1 = 0.0f, gC2 = 0.0f;
       uint32_t st0 = 0, st1 = 0, st2 = 0;
       int32_t cg6 = 0, cg7 = 0;
       if (inside) {
@@ -248,8 +248,7 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
           const float D2 = 9.0000000000000003e-04f;  // f32(0.03 * 0.03), a WGSL const-expression
           const float rt0 = sqrtf(er0 * er0 + D2), rt1 = sqrtf(er1 * er1 + D2), rt2 = sqrtf(er2 * er2 + D2);
           const float eg0 = er0 / rt0, eg1 = er1 / rt1, eg2 = er2 / rt2;
-          gC0 = gain * eg0; gC1 = gain * eg1; gC2 = gain * eg2;
-          g16_0 = gC0 * FIXED; g16_1 = gC1 * FIXED; g16_2 = gC2 * FIXED;
+          g16_0 = (gain * eg0) * FIXED; g16_1 = (gain * eg1) * FIXED; g16_2 = (gain * eg2) * FIXED;
           const float lossv = (rt0 + rt1 + rt2) - 8.9999999999999997e-02f;  // f32(3 * 0.03)
           st1 = u32sat(lossv * 32768.0f);
           cg6 = fixq((eg0 * C0 + eg1 * C1 + eg2 * C2) * gain, FIXCAM);
@@ -333,9 +332,8 @@ __global__ void __launch_bounds__(TILE * TILE, TILE == 16 ? GS_RASTER16_MIN_BLOC
             const float g0 = __fmaf_rn(r1.z, Tb, -(S0 * inv));
             const float g1 = __fmaf_rn(r1.w, Tb, -(S1 * inv));
             const float g2 = __fmaf_rn(r2.x, Tb, -(S2 * inv));
-            float galpha = __fmaf_rn(gC2, g2, __fmaf_rn(gC1, g1, gC0 * g0));
-            if (araw > 0.99f) galpha = 0.0f;
-            const float gal16 = c2 ? galpha * FIXED : 0.0f;
+            // galpha * 2^14, accumulated from gC * 2^14
+            const float gal16 = c2 && !(araw > 0.99f) ? __fmaf_rn(g16_2, g2, __fmaf_rn(g16_1, g1, g16_0 * g0)) : 0.0f;
             const float ga16 = gal16 * araw;
             const float cA = r0.z + r0.z, cC = r1.x + r1.x;  // exact doubling of the stored halves
             const float gq16 = ga16 * r2.z;  // r2.z = -cnorm / 2
@@ -423,7 +421,7 @@ __device__ __forceinline__ float2 pairExponent2(const float4& r0, float hC, floa
 }
 
 #ifndef GS_RASTER_PX2_MIN_BLOCKS
-#define GS_RASTER_PX2_MIN_BLOCKS 7  // resident 128-thread blocks per SM the register allocation must allow
+#define GS_RASTER_PX2_MIN_BLOCKS 8  // resident 128-thread blocks per SM the register allocation must allow
 #endif
 // Fused train tile (forward + loss + backward) on a 16x16 tile with two
 // pixels per thread: 128 threads, each warp covering an 8x8 block; lane l
@@ -574,7 +572,6 @@ __global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(Ra
     }
 
     // ---- loss (shaders.js:589-618), per pixel ----
-    float2 gC0 = bc2(0.0f), gC1 = bc2(0.0f), gC2 = bc2(0.0f);
     float2 g16_0 = bc2(0.0f), g16_1 = bc2(0.0f), g16_2 = bc2(0.0f);
     uint32_t st0 = 0, st1 = 0, st2 = 0, cg6 = 0, cg7 = 0;
     uint32_t myEndA = 0, myEndB = 0;
@@ -605,11 +602,9 @@ __global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(Ra
       cg6 += (uint32_t)fixq((eg0 * Cx + eg1 * Cy + eg2 * Cz) * gain, FIXCAM);
       cg7 += (uint32_t)fixq(eg0 + eg1 + eg2, FIXCAM);
       if (h) {
-        gC0.y = q0; gC1.y = q1; gC2.y = q2;
         g16_0.y = q0 * FIXED; g16_1.y = q1 * FIXED; g16_2.y = q2 * FIXED;
         myEndB = cntB;
       } else {
-        gC0.x = q0; gC1.x = q1; gC2.x = q2;
         g16_0.x = q0 * FIXED; g16_1.x = q1 * FIXED; g16_2.x = q2 * FIXED;
         myEndA = cntA;
       }
@@ -687,8 +682,8 @@ __global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(Ra
           const float2 g0 = __ffma2_rn(bc2(r1.z), Tb, __fmul2_rn(make_float2(-S0.x, -S0.y), inv));
           const float2 g1 = __ffma2_rn(bc2(r1.w), Tb, __fmul2_rn(make_float2(-S1.x, -S1.y), inv));
           const float2 g2 = __ffma2_rn(bc2(r2.x), Tb, __fmul2_rn(make_float2(-S2.x, -S2.y), inv));
-          const float2 gal = __ffma2_rn(gC2, g2, __ffma2_rn(gC1, g1, __fmul2_rn(gC0, g0)));
-          const float2 gal16r = __fmul2_rn(gal, bc2(FIXED));
+          // galpha * 2^14, accumulated from gC * 2^14
+          const float2 gal16r = __ffma2_rn(g16_2, g2, __ffma2_rn(g16_1, g1, __fmul2_rn(g16_0, g0)));
           const float2 gal16 = make_float2(c2a && !(araw.x > 0.99f) ? gal16r.x : 0.0f,
                                            c2b && !(araw.y > 0.99f) ? gal16r.y : 0.0f);
           const float2 ga16 = __fmul2_rn(gal16, araw);
