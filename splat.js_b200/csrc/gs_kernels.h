@@ -206,7 +206,8 @@ void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s);
 void launch_raster(const RasterArgs& a, int mode, bool stored, int tile, int batchDepth, unsigned grid,
                    cudaStream_t s);
 int raster_blocks_per_sm(int tile, int batchDepth, int mode);
-void launch_work_order(const uint2* ranges, uint32_t totalTiles, uint32_t* order, cudaStream_t s);
+void launch_work_order(const uint2* ranges, uint32_t totalTiles, uint32_t* order, uint32_t* scratch,
+                       cudaStream_t s);
 void launch_chain_adam(const ChainArgs& a, int deg, cudaStream_t s);
 void launch_refine_classify(const float* params, uint32_t n, uint32_t* deadFlag, uint32_t* donorFlag,
                             cudaStream_t s);

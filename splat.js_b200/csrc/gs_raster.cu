@@ -811,43 +811,62 @@ int raster_blocks_per_sm(int tile, int batchDepth, int mode) {
 }
 
 // Work order for the persistent queue: global tiles by descending entry
-// count (bucketed by log2), so the heaviest tiles start first.
-__global__ void __launch_bounds__(1024) k_work_order(const uint2* ranges, uint32_t totalTiles, uint32_t* order) {
-  __shared__ uint32_t s_hist[33];
-  __shared__ uint32_t s_off[33];
-  if (threadIdx.x < 33) s_hist[threadIdx.x] = 0;
-  __syncthreads();
-  // most tiles fall in a few buckets: one shared atomic per bucket per warp
-  // (whole warps step through the tiles; lanes past the end use bucket 64)
+// count (bucketed by log2), so the heaviest tiles start first.  Three small
+// grid-wide kernels: bucket sizes, their exclusive scan, and the placement of
+// every tile at its bucket's cursor.  The order inside a bucket follows the
+// cursor atomics; no result depends on it (tiles write disjoint pixels and
+// integer gradient sums), only the schedule does.
+__device__ __forceinline__ uint32_t tile_bucket(const uint2* ranges, uint32_t t) {
+  return (uint32_t)__clz(ranges[t].y - ranges[t].x);  // 32: empty, 0: longest
+}
+
+// one atomic per bucket per warp (whole warps step through the tiles; lanes
+// past the end use bucket 64)
+__global__ void __launch_bounds__(1024) k_work_count(const uint2* ranges, uint32_t totalTiles, uint32_t* counts) {
   const uint32_t lane = threadIdx.x & 31u;
-  for (uint32_t t0 = threadIdx.x - lane; t0 < totalTiles; t0 += blockDim.x) {
-    const uint32_t t = t0 + lane;
-    const bool valid = t < totalTiles;
-    const uint32_t b = valid ? (uint32_t)__clz(ranges[t].y - ranges[t].x) : 64u;  // 32: empty, 0: longest
-    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, b);
-    if (valid && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&s_hist[b], (uint32_t)__popc(peers));
-  }
-  __syncthreads();
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = t < totalTiles;
+  const uint32_t b = valid ? tile_bucket(ranges, t) : 64u;
+  const uint32_t peers = __match_any_sync(0xFFFFFFFFu, b);
+  if (valid && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&counts[b], (uint32_t)__popc(peers));
+}
+
+// cursors = exclusive scan of the 33 bucket sizes; the sizes are cleared for
+// the next use
+__global__ void k_work_scan(uint32_t* counts, uint32_t* cursors) {
   if (threadIdx.x == 0) {
     uint32_t acc = 0;
-    for (int b = 0; b < 33; ++b) { s_off[b] = acc; acc += s_hist[b]; }
-  }
-  __syncthreads();
-  for (uint32_t t0 = threadIdx.x - lane; t0 < totalTiles; t0 += blockDim.x) {
-    const uint32_t t = t0 + lane;
-    const bool valid = t < totalTiles;
-    const uint32_t b = valid ? (uint32_t)__clz(ranges[t].y - ranges[t].x) : 64u;
-    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, b);
-    const uint32_t lead = (uint32_t)(__ffs(peers) - 1);
-    uint32_t base = 0;
-    if (valid && lane == lead) base = atomicAdd(&s_off[b], (uint32_t)__popc(peers));
-    base = __shfl_sync(0xFFFFFFFFu, base, lead);
-    if (valid) order[base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = t;
+    for (int b = 0; b < 33; ++b) {
+      cursors[b] = acc;
+      acc += counts[b];
+      counts[b] = 0u;
+    }
   }
 }
 
-void launch_work_order(const uint2* ranges, uint32_t totalTiles, uint32_t* order, cudaStream_t s) {
-  k_work_order<<<1, 1024, 0, s>>>(ranges, totalTiles, order);
+__global__ void __launch_bounds__(1024) k_work_place(const uint2* ranges, uint32_t totalTiles, uint32_t* cursors,
+                                                     uint32_t* order) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = t < totalTiles;
+  const uint32_t b = valid ? tile_bucket(ranges, t) : 64u;
+  const uint32_t peers = __match_any_sync(0xFFFFFFFFu, b);
+  const uint32_t lead = (uint32_t)(__ffs(peers) - 1);
+  uint32_t base = 0;
+  if (valid && lane == lead) base = atomicAdd(&cursors[b], (uint32_t)__popc(peers));
+  base = __shfl_sync(0xFFFFFFFFu, base, lead);
+  if (valid) order[base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = t;
+}
+
+// scratch: 66 words, the first 33 zero before the first call (each call
+// leaves them zero)
+void launch_work_order(const uint2* ranges, uint32_t totalTiles, uint32_t* order, uint32_t* scratch,
+                       cudaStream_t s) {
+  if (totalTiles == 0) return;
+  const unsigned blocks = (totalTiles + 1023) / 1024;
+  k_work_count<<<blocks, 1024, 0, s>>>(ranges, totalTiles, scratch);
+  k_work_scan<<<1, 32, 0, s>>>(scratch, scratch + 33);
+  k_work_place<<<blocks, 1024, 0, s>>>(ranges, totalTiles, scratch + 33, order);
 }
 
 }  // namespace gs

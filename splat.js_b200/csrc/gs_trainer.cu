@@ -684,13 +684,13 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   if (cull) launch_ranges_from_keys(h->keys[passes & 1], totalEntries, totalTiles, h->ranges, s);
   // kernels: project, tile counts + finish, presort (histogram + passes),
   // entry counts, 3 scan kernels, entry keys, tile sort (histogram +
-  // passes), [ranges from keys], [work order], raster, [visible lists, chain per view, sum + Adam]
+  // passes), [ranges from keys], [work order: 3], raster, [visible lists, chain per view, sum + Adam]
   h->lastLaunches = 3u + 1u + (uint32_t)pr.passes + 1u + 3u + 1u + 1u + (uint32_t)passes + (cull ? 1u : 0u) +
-                    (h->o.persistent ? 1u : 0u) + 1u + (sh.chain ? 3u : 0u);
+                    (h->o.persistent ? 3u : 0u) + 1u + (sh.chain ? 3u : 0u);
   const uint32_t* sortedIds = h->vals[passes & 1];
 
   const bool persistent = h->o.persistent != 0;
-  if (persistent) launch_work_order(h->ranges, totalTiles, h->workOrder, s);
+  if (persistent) launch_work_order(h->ranges, totalTiles, h->workOrder, h->small + 2080, s);  // [2080, 2146)
   if (h->profiling) cudaEventRecord(ph[2], s);
   RasterArgs rr{};
   rr.cams = dcams;
