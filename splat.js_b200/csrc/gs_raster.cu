@@ -674,7 +674,8 @@ __global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(Ra
           const float2 alpha = make_float2(fminf(0.99f, araw.x), fminf(0.99f, araw.y));
           const bool c2a = j < myEndA && ee.x <= E_CUT && alpha.x >= A_MIN;
           const bool c2b = j < myEndB && ee.y <= E_CUT && alpha.y >= A_MIN;
-          if (!__any_sync(FULL, c2a || c2b)) continue;
+          const uint32_t balA = __ballot_sync(FULL, c2a), balB = __ballot_sync(FULL, c2b);
+          if ((balA | balB) == 0u) continue;
           const float2 inv = rcp_unit2(__fadd2_rn(bc2(1.0f), make_float2(-alpha.x, -alpha.y)));
           const float2 Tb = __fmul2_rn(Ta, inv);
           const float2 at = __fmul2_rn(alpha, Tb);
@@ -707,9 +708,18 @@ __global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(Ra
             for (int k = 0; k < 10; ++k)
               xs[k] = make_float2(fminf(fmaxf(xs[k].x, -1.0e9f), 1.0e9f), fminf(fmaxf(xs[k].y, -1.0e9f), 1.0e9f));
           }
+          // a half of the block with no compositing pixel has every value 0
+          if (balA != 0u && balB != 0u) {
 #pragma unroll
-          for (int k = 0; k < 10; ++k)
-            rsum[k] = __reduce_add_sync(FULL, (uint32_t)__float2int_rz(xs[k].x) + (uint32_t)__float2int_rz(xs[k].y));
+            for (int k = 0; k < 10; ++k)
+              rsum[k] = __reduce_add_sync(FULL, (uint32_t)__float2int_rz(xs[k].x) + (uint32_t)__float2int_rz(xs[k].y));
+          } else if (balA != 0u) {
+#pragma unroll
+            for (int k = 0; k < 10; ++k) rsum[k] = __reduce_add_sync(FULL, (uint32_t)__float2int_rz(xs[k].x));
+          } else {
+#pragma unroll
+            for (int k = 0; k < 10; ++k) rsum[k] = __reduce_add_sync(FULL, (uint32_t)__float2int_rz(xs[k].y));
+          }
           // a pixel that does not composite has aT = 0: S stays exactly as it is
           S0 = __ffma2_rn(bc2(r1.z), aT, S0);
           S1 = __ffma2_rn(bc2(r1.w), aT, S1);
