@@ -168,13 +168,14 @@ def oracle_adam(t, iter_after, radius, horizon=60000, opacityReg=0.01, shLr=1.25
                      float(np.float32(math.log(radius * 0.05))), reg=opacityReg, shLr=shLr)
 
 
-@pytest.mark.parametrize("cull,depth", [(1, 64), (0, 64), (1, 128), (1, 256)])
-def test_config0_raster_bitexact(cull, depth):
+@pytest.mark.parametrize("cull,depth,persistent", [(1, 64, 1), (0, 64, 1), (1, 128, 1), (1, 256, 1), (1, 256, 0)])
+def test_config0_raster_bitexact(cull, depth, persistent):
     """cull=0: the reference's full rectangle lists, per-tile order included;
-    depth: entries staged per shared-memory batch of the fused raster."""
+    depth: entries staged per shared-memory batch of the fused raster;
+    persistent=0: one block per tile instead of the persistent work queue."""
     params, sh, cams, rgbs = config0()
     n = len(params) // 16
-    opts = dict(shDeg=2, tileCull=cull, batchDepth=depth)
+    opts = dict(shDeg=2, tileCull=cull, batchDepth=depth, persistent=persistent)
     t, targets, metas = make(params, sh, cams, rgbs, opts, radius=1.0)
     gpu_raster(t, [0], 3)
     check_view_against_oracle(t, oracle_opts(opts), oracle_cam(metas[0], 0, 1, 2), params, sh, targets, n)
