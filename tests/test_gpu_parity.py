@@ -504,6 +504,31 @@ def test_full_size_views_bitexact():
     assert_bits(g["sh"], s, "SH after a full-size batched step")
 
 
+def test_full_size_deg3_bitexact():
+    """Config 4's scene at full size: 2M splats at SH degree 3 (K = 15), a
+    fifth of them fine (log-scale N(-7, 0.5)), one 1920x1080 view: every
+    record, list, pixel and gradient, then one optimiser step."""
+    n = 2_000_000
+    params, sh = scene.surface_scene(n, seed=4, sh_deg=3, log_scale=(-5.0, 0.7), fine_frac=0.2)
+    cams = [scene.ring_cameras(24, 4.0, 0.5, 1920, 1080)[3]]
+    rgbs = [scene.uniform_target(1920, 1080, seed=11)]
+    opts = dict(shDeg=3, maxSplats=n, batchDepth=256, entriesCap=24 * n)
+    t, targets, metas = make(params, sh, cams, rgbs, opts, radius=4.0)
+    t.iter = 3000  # the SH ramp (one band per 1000 iterations) has every band active
+    gpu_raster(t, [0], 3)
+    o = oracle_opts(opts)
+    check_view_against_oracle(t, o, oracle_cam(metas[0], 0, 1, 3), params, sh, targets, n)
+    K = 15
+    m, vv = np.zeros(n * 16, np.float32), np.zeros(n * 16, np.float32)
+    sm, sv = np.zeros(n * 3 * K, np.float32), np.zeros(n * 3 * K, np.float32)
+    p, s = params.copy(), sh.copy()
+    t.stepBatch([0])
+    O.step(o, [oracle_cam(metas[0], 0, 1, 3)], oracle_adam(t, 3001, 4.0), p, s, targets, m, vv, sm, sv, n)
+    g = t.readGaussians()
+    assert_bits(g["data"], p, "params after a degree-3 full-size step")
+    assert_bits(g["sh"], s, "SH after a degree-3 full-size step")
+
+
 def test_lookback_timeout_is_reported_and_device_stays_usable():
     """A sort pass whose look-back can never complete gives up after a bounded
     number of spins, sets the timeout bit, and leaves the device usable."""
