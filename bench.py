@@ -40,7 +40,7 @@ METRIC = "train views/s @1M splats 1080p, batched vs plain step, 1 B200, grads w
 FLOP_PER_PAIR = 26 + 70   # raster forward + backward per evaluated pixel-entry pair (FFMA = 2)
 # DRAM bytes (read + write) of one raster launch over an 8-view batch at the
 # default workload, from one ncu capture (not measured live)
-RASTER_DRAM_BYTES_8VIEW = 1.152209e9 + 0.460524e9
+RASTER_DRAM_BYTES_8VIEW = 2.009056e9 + 0.522827e9
 
 
 def parse():
@@ -373,6 +373,9 @@ def run_ours(args):
         for k in range(steps):
             fn(k)
         e1.record(stream)
+        # wait in the library (ctypes drops the GIL), so the clock sampler's
+        # thread keeps sampling while the device works
+        N.check(L.gs_sync(h), h)
         barrier()
         ms = max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{local}")
         return ms, job_rate(views_per_step, steps, world, ms)
