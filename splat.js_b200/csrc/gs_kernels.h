@@ -50,7 +50,7 @@ struct ExpandArgs {
   const RenderRec* recs;        // read when cull != 0 (the mean)
   const float4* cullRecs;       // read when cull != 0
   uint4* itemRecs;              // V * n * 2: per presorted item (rect, mean, cull parameters, slot)
-  const uint32_t* presortHist;  // the presort's digit histograms (4 x 256): culled items = [3 * 256 + 255]
+  const uint32_t* liveItems;    // presorted items kept (the culled ones left the presort)
   const uint8_t* dropped;
   const uint32_t* viewDrops;
   float eCut, aMin;
@@ -70,6 +70,7 @@ struct RadixHistArgs {
   uint32_t* hist;           // passes * 256
   int passes;
   uint32_t* epoch;
+  uint32_t* nKept;          // non-null: all-ones keys are dropped (not counted); kept keys are counted here
 };
 
 #ifndef GS_SORT_ITEMS
@@ -90,6 +91,8 @@ struct OnesweepArgs {
   const uint32_t* epoch;
   int pass;
   uint32_t spinLimit;       // look-back spins before the block gives up and flags a timeout
+  int dropAllOnes;          // all-ones keys leave the sort (output compacted to the kept keys);
+                            // selects the kernel instantiation that drops them
 };
 
 struct RadixSortArgs {
@@ -105,6 +108,8 @@ struct RadixSortArgs {
   int passes;
   bool keepKeys;
   unsigned histGrid, sweepGrid;
+  uint32_t* nKept;          // non-null (32-bit keys): all-ones keys are dropped in the first pass and the
+                            // kept count lands here (zero before the call); later passes sort only those
 };
 
 struct RasterArgs {

@@ -319,10 +319,9 @@ template <bool KEYS>
 __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
   __shared__ uint32_t s_run[256];  // entries of each item so far
   const uint64_t items = (uint64_t)a.n * a.V;
-  // culled items carry the all-ones key, the only key whose top byte is 0xFF
-  // (depth bits of a positive float are below 0x7F800000): the presort puts
-  // them last and its top-digit histogram counts them
-  const uint64_t live = items - a.presortHist[3 * 256 + 255];
+  // culled items carry the all-ones key, which the presort drops: its output
+  // holds the live items only
+  const uint64_t live = *a.liveItems;
   const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if ((uint64_t)blockIdx.x * blockDim.x >= live) {  // the whole block is culled items (uniform)
     if (!KEYS && p < items) a.counts[p] = 0u;

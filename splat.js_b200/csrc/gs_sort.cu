@@ -140,8 +140,9 @@ constexpr int RS_MAX_PASSES = 8;
 constexpr uint32_t FLAG_AGG = 1u, FLAG_INC = 2u;
 constexpr uint32_t LOOKBACK_SPIN_LIMIT = 1u << 22;
 
-// Histogram of every digit position: one read of all keys.
-template <typename KT>
+// Histogram of every digit position: one read of all keys (DROP: all-ones
+// keys are not counted; the kept ones are counted into nKept).
+template <typename KT, bool DROP>
 __global__ void __launch_bounds__(256) k_radix_hist(RadixHistArgs a) {
   __shared__ uint32_t h[RS_MAX_PASSES][256];
   for (int i = threadIdx.x; i < RS_MAX_PASSES * 256; i += blockDim.x) (&h[0][0])[i] = 0;
@@ -150,20 +151,30 @@ __global__ void __launch_bounds__(256) k_radix_hist(RadixHistArgs a) {
   const KT* keys = static_cast<const KT*>(a.keys);
   // four keys per thread in flight, then their digits counted
   const uint32_t stride = gridDim.x * blockDim.x;
+  const KT ALL = ~KT(0);
+  uint32_t kept = 0;
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   for (; i + 3 * stride < N; i += 4 * stride) {
     const KT k0 = keys[i], k1 = keys[i + stride], k2 = keys[i + 2 * stride], k3 = keys[i + 3 * stride];
+    const bool u0 = !DROP || k0 != ALL, u1 = !DROP || k1 != ALL, u2 = !DROP || k2 != ALL, u3 = !DROP || k3 != ALL;
+    kept += (uint32_t)u0 + (uint32_t)u1 + (uint32_t)u2 + (uint32_t)u3;
     for (int p = 0; p < a.passes; ++p) {
       const int sh = 8 * p;
-      atomicAdd(&h[p][(k0 >> sh) & 0xFF], 1u);
-      atomicAdd(&h[p][(k1 >> sh) & 0xFF], 1u);
-      atomicAdd(&h[p][(k2 >> sh) & 0xFF], 1u);
-      atomicAdd(&h[p][(k3 >> sh) & 0xFF], 1u);
+      if (u0) atomicAdd(&h[p][(k0 >> sh) & 0xFF], 1u);
+      if (u1) atomicAdd(&h[p][(k1 >> sh) & 0xFF], 1u);
+      if (u2) atomicAdd(&h[p][(k2 >> sh) & 0xFF], 1u);
+      if (u3) atomicAdd(&h[p][(k3 >> sh) & 0xFF], 1u);
     }
   }
   for (; i < N; i += stride) {
     const KT k = keys[i];
+    if (DROP && k == ALL) continue;
+    ++kept;
     for (int p = 0; p < a.passes; ++p) atomicAdd(&h[p][(k >> (8 * p)) & 0xFF], 1u);
+  }
+  if (DROP) {
+    const uint32_t wk = __reduce_add_sync(0xFFFFFFFFu, kept);
+    if ((threadIdx.x & 31) == 0 && wk) atomicAdd(a.nKept, wk);
   }
   __syncthreads();
   for (int p = 0; p < a.passes; ++p)
@@ -178,7 +189,7 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   return m;
 }
 
-template <typename KT>
+template <typename KT, bool DROP = false>
 #ifndef GS_SORT_MIN_BLOCKS
 #define GS_SORT_MIN_BLOCKS 3  // resident blocks per SM the register allocation must allow
 #endif
@@ -245,7 +256,7 @@ __global__ void __launch_bounds__(RS_THREADS, GS_SORT_MIN_BLOCKS) k_onesweep(One
       if (idx < N) {
         key[j] = keysIn[idx];
         val[j] = a.valsIn[idx];
-        dig[j] = (uint32_t)(key[j] >> shift) & 0xFFu;
+        dig[j] = DROP && key[j] == ~KT(0) ? 0x100u : (uint32_t)(key[j] >> shift) & 0xFFu;
       } else {
         key[j] = 0; val[j] = 0; dig[j] = 0x100u;
       }
@@ -391,7 +402,8 @@ __global__ void __launch_bounds__(RS_THREADS, GS_SORT_MIN_BLOCKS) k_onesweep(One
       s_gbase[d] = s_dbase[d] + excl;
     }
     __syncthreads();
-    const uint32_t cnt = min((uint32_t)RS_TILE, N - base);
+    // the block's entries (DROP: the kept ones), staged first to last
+    const uint32_t cnt = DROP ? s_local[255] + s_run[255] : min((uint32_t)RS_TILE, N - base);
     for (uint32_t i = tid; i < cnt; i += RS_THREADS) {
       const KT k = s_keys[i];
       const uint32_t d = (uint32_t)(k >> shift) & 0xFFu;
@@ -410,6 +422,8 @@ int onesweep_grid(int device) {
   int sms = 0, per32 = 0, per64 = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   cudaFuncSetAttribute(k_onesweep<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)rs_dyn_smem<uint32_t>());
+  cudaFuncSetAttribute(k_onesweep<uint32_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)rs_dyn_smem<uint32_t>());
   cudaFuncSetAttribute(k_onesweep<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)rs_dyn_smem<uint64_t>());
@@ -432,14 +446,20 @@ static void radix_sort_t(const RadixSortArgs& a, cudaStream_t s) {
   h.hist = a.hist;
   h.passes = a.passes;
   h.epoch = a.epoch;
-  k_radix_hist<KT><<<a.histGrid, 256, 0, s>>>(h);
+  const bool drop = a.nKept != nullptr && sizeof(KT) == 4;
+  h.nKept = drop ? a.nKept : nullptr;
+  if (drop) k_radix_hist<KT, true><<<a.histGrid, 256, 0, s>>>(h);
+  else k_radix_hist<KT, false><<<a.histGrid, 256, 0, s>>>(h);
   for (int p = 0; p < a.passes; ++p) {
     OnesweepArgs o;
     o.keysIn = a.keys[p & 1];
     o.valsIn = a.vals[p & 1];
     o.keysOut = (p == a.passes - 1 && !a.keepKeys) ? nullptr : a.keys[(p + 1) & 1];
     o.valsOut = a.vals[(p + 1) & 1];
-    o.nItems = a.nItems;
+    // the first pass reads every key and drops the all-ones ones; the later
+    // passes sort only the kept keys
+    o.nItems = drop && p > 0 ? a.nKept : a.nItems;
+    o.dropAllOnes = drop && p == 0 ? 1 : 0;
     o.hist = a.hist;
     o.tileCounter = a.tileCounter;
     o.status = a.status;
@@ -447,7 +467,8 @@ static void radix_sort_t(const RadixSortArgs& a, cudaStream_t s) {
     o.epoch = a.epoch;
     o.pass = p;
     o.spinLimit = LOOKBACK_SPIN_LIMIT;
-    k_onesweep<KT><<<a.sweepGrid, RS_THREADS, rs_dyn_smem<KT>(), s>>>(o);
+    if (o.dropAllOnes) k_onesweep<KT, true><<<a.sweepGrid, RS_THREADS, rs_dyn_smem<KT>(), s>>>(o);
+    else k_onesweep<KT><<<a.sweepGrid, RS_THREADS, rs_dyn_smem<KT>(), s>>>(o);
   }
 }
 
@@ -489,11 +510,13 @@ int debug_lookback_timeout(int device, uint32_t spinLimit, uint32_t* statusOut, 
     cudaMemcpyAsync(small + 2058, &n, 4, cudaMemcpyHostToDevice, s);
     RadixHistArgs h;
     h.keys = keys; h.nItems = small + 2058; h.hist = small; h.passes = 1; h.epoch = small + 2057;
-    k_radix_hist<uint32_t><<<4, 256, 0, s>>>(h);
+    h.nKept = nullptr;
+    k_radix_hist<uint32_t, false><<<4, 256, 0, s>>>(h);
     OnesweepArgs o;
     o.keysIn = keys; o.valsIn = vals; o.keysOut = nullptr; o.valsOut = outVals;
     o.nItems = small + 2058; o.hist = small; o.tileCounter = small + 2048; o.status = status;
     o.statusWord = small + 2056; o.epoch = small + 2057; o.pass = 0; o.spinLimit = spinLimit;
+    o.dropAllOnes = 0;
     cudaFuncSetAttribute(k_onesweep<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)rs_dyn_smem<uint32_t>());
     cudaEventRecord(e0, s);

@@ -629,6 +629,11 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   pr.keepKeys = false;
   pr.histGrid = (unsigned)h->histGrid;
   pr.sweepGrid = (unsigned)h->sweepGrid;
+  // culled items (all-ones keys) leave the presort: only the visible ones
+  // are sorted, and their count sizes the expansion
+  uint32_t* liveItems = h->small + 2150;
+  pr.nKept = liveItems;
+  cudaMemsetAsync(liveItems, 0, 4, s);
   if (h->profiling) cudaEventRecord(ph[1], s);
   launch_radix_sort(pr, s);
   const uint32_t* sortedSlots = h->pvals[pr.passes & 1];
@@ -643,7 +648,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   ea.recs = h->recs;
   ea.cullRecs = h->cullRecs;
   ea.itemRecs = h->itemRecs;
-  ea.presortHist = hist;
+  ea.liveItems = liveItems;
   ea.dropped = h->dropped;
   ea.viewDrops = h->viewDrops;
   ea.eCut = h->o.eCut;
