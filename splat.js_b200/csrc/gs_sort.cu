@@ -404,12 +404,18 @@ __global__ void __launch_bounds__(RS_THREADS, GS_SORT_MIN_BLOCKS) k_onesweep(One
     __syncthreads();
     // the block's entries (DROP: the kept ones), staged first to last
     const uint32_t cnt = DROP ? s_local[255] + s_run[255] : min((uint32_t)RS_TILE, N - base);
-    for (uint32_t i = tid; i < cnt; i += RS_THREADS) {
-      const KT k = s_keys[i];
-      const uint32_t d = (uint32_t)(k >> shift) & 0xFFu;
-      const uint32_t g = s_gbase[d] + (i - s_local[d]);
-      if (keysOut) keysOut[g] = k;
-      a.valsOut[g] = s_vals[i];
+    // scatter, every round unrolled so the shared-memory reads of all rounds
+    // are in flight together
+#pragma unroll
+    for (int r = 0; r < RS_ITEMS; ++r) {
+      const uint32_t i = (uint32_t)tid + (uint32_t)r * RS_THREADS;
+      if (i < cnt) {
+        const KT k = s_keys[i];
+        const uint32_t d = (uint32_t)(k >> shift) & 0xFFu;
+        const uint32_t g = s_gbase[d] + (i - s_local[d]);
+        if (keysOut) keysOut[g] = k;
+        a.valsOut[g] = s_vals[i];
+      }
     }
     __syncthreads();
   }
