@@ -40,7 +40,7 @@ METRIC = "train views/s @1M splats 1080p, batched vs plain step, 1 B200, grads w
 FLOP_PER_PAIR = 26 + 70   # raster forward + backward per evaluated pixel-entry pair (FFMA = 2)
 # DRAM bytes (read + write) of one raster launch over an 8-view batch at the
 # default workload, from one ncu capture (not measured live)
-RASTER_DRAM_BYTES_8VIEW = 2.009056e9 + 0.522827e9
+RASTER_DRAM_BYTES_8VIEW = 2.013450e9 + 0.524951e9
 
 
 def parse():
