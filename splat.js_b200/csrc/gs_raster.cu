@@ -753,7 +753,7 @@ __global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(Ra
 
 template <int TILE, int BATCH, bool FWD, bool BWD, bool STORED>
 static void launch_one(const RasterArgs& a, unsigned grid, cudaStream_t s) {
-  if (TILE == 16 && FWD && BWD && !STORED) k_raster_px2<BATCH><<<grid, 128, 0, s>>>(a);
+  if constexpr (TILE == 16 && FWD && BWD && !STORED) k_raster_px2<BATCH><<<grid, 128, 0, s>>>(a);
   else k_raster<TILE, BATCH, FWD, BWD, STORED><<<grid, TILE * TILE, 0, s>>>(a);
 }
 
