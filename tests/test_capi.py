@@ -75,3 +75,20 @@ def test_lookback_check_rejects_bad_spin_limits():
     st, ms = C.c_uint32(), C.c_double()
     assert N.lib().gs_debug_lookback_timeout(0, 0, C.byref(st), C.byref(ms)) == -1
     assert N.lib().gs_debug_lookback_timeout(0, (1 << 22) + 1, C.byref(st), C.byref(ms)) == -1
+
+
+def test_ingestion_entry_points_check_their_arguments():
+    """gs_undistort_frames and gs_debug_targets refuse bad arguments before
+    touching a device; below the distortion noise floor nothing is resampled
+    and no device is needed."""
+    L = N.lib()
+    done = C.c_int32(7)
+    assert L.gs_undistort_frames(0, None, 1, 0.3, 0.0, 10.0, C.byref(done)) == -1
+    assert done.value == 0
+    fr = (N.GsFrame * 1)()
+    fr[0].tw, fr[0].th, fr[0].fw = 4, 4, 4.0          # pixels but no buffer
+    assert L.gs_undistort_frames(0, fr, 1, 0.3, 0.0, 10.0, C.byref(done)) == -1
+    done.value = 7
+    assert L.gs_undistort_frames(0, fr, 1, 0.005, -0.005, 10.0, C.byref(done)) == 0
+    assert done.value == 0
+    assert L.gs_debug_targets(None, None, 0) == -1
