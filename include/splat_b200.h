@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define GS_ABI_VERSION 1
+#define GS_ABI_VERSION 2  /* 2: gs_options.donorSampling */
 
 #if defined(__GNUC__)
 #define GS_API __attribute__((visibility("default")))
@@ -70,6 +70,9 @@ typedef struct gs_options {
   int32_t device;          /* CUDA device ordinal */
   int32_t tileCull;        /* 1: tile lists keep only entries whose splat can reach a pixel of the tile
                               (exact ellipse/tile test); images and gradients are identical either way */
+  int32_t donorSampling;   /* refine's clone donors: 0 uniform over the donors (the reference,
+                              trainer.js:722); 1 opacity-weighted (probability proportional to
+                              sigmoid(opacity logit)), one rng() draw per pick either way */
 } gs_options;
 
 /* One camera of setup's cams[] (trainer.js:95-99) with the exposure state
@@ -186,7 +189,8 @@ GS_API int gs_read_cam_grads(gs_trainer* h, int32_t* out, int32_t reset);
 
 /* refine(rng) (trainer.js:666-794): dead/donor classification, donor order
  * and the parameter writes run on the device; only rng() draws are made on
- * the host, in the reference's order. */
+ * the host, in the reference's order.  gs_options.donorSampling = 1 picks
+ * clone donors by opacity weight from the same draws. */
 GS_API int gs_refine(gs_trainer* h, gs_rng_fn rng, void* ctx, gs_refine_result* out);
 /* device.queue.onSubmittedWorkDone() (session.js:520, 542): waits for the stream. */
 GS_API int gs_sync(gs_trainer* h);

@@ -90,7 +90,7 @@ def lib():
         L.oracle_eval_f64.argtypes = [P(OOpts), P(OCam), f64p, f64p, C.c_uint32, u32p, f64p, f64p, f64p, f32p]
         L.oracle_refine.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double,
                                     C.c_int, f32p, f32p, f32p, f32p, f32p, f32p, RNG_FN, C.c_void_p,
-                                    P(ORefineOut)]
+                                    P(ORefineOut), C.c_int]
         _lib = L
     return _lib
 
@@ -233,15 +233,18 @@ def eval_f64(o, c, params64, sh64, n, targets, grads=True, want_image=False):
     return loss3, gF, (sG[: n * 3 * K] if grads else None), img
 
 
-def refine(n, cap, params, m, v, sh, shM, shV, K, rng, iter_, growUntil, growRate=0.15, growLimit=0):
-    """MCMC-lite refine (trainer.js:666-794) in place; rng() -> float in [0,1)."""
+def refine(n, cap, params, m, v, sh, shM, shV, K, rng, iter_, growUntil, growRate=0.15, growLimit=0,
+           donorSampling=0):
+    """MCMC-lite refine (trainer.js:666-794) in place; rng() -> float in [0,1).
+    donorSampling 1 picks clone donors by opacity weight (no reference
+    counterpart; the reference samples uniformly, trainer.js:722)."""
     cb = RNG_FN(lambda _ctx: float(rng()))
     out = ORefineOut()
     dummy = np.zeros(1, np.float32)
     lib().oracle_refine(n, cap, growLimit, float(iter_), float(growUntil), float(growRate), K,
                         _p(params, C.c_float), _p(m, C.c_float), _p(v, C.c_float),
                         _p(sh if K else dummy, C.c_float), _p(shM if K else dummy, C.c_float),
-                        _p(shV if K else dummy, C.c_float), cb, None, C.byref(out))
+                        _p(shV if K else dummy, C.c_float), cb, None, C.byref(out), int(donorSampling))
     return dict(moved=out.moved, grown=out.grown, n=out.n, early=bool(out.early))
 
 

@@ -286,12 +286,15 @@ void oracle_eval_f64(const OOpts* oo, const OCam* oc, const double* params, cons
 // params/m/v are cap*16 f32, sh/shM/shV cap*3K f32.  rng() returns doubles
 // in [0,1) in the order the reference draws them.  JS arithmetic is double;
 // Float32Array stores round to f32, which the casts below reproduce.
+// donorSampling 1 (no reference counterpart): a clone's donor is the first
+// whose cumulative sigmoid(opacity) over the donor list exceeds rng() * total,
+// the same single draw the uniform pick makes.
 typedef double (*oracle_rng_fn)(void*);
 struct ORefineOut { uint32_t moved, grown, n; int32_t early; };
 
 void oracle_refine(uint32_t n, uint32_t cap, uint32_t growLimit, double iter, double growUntil, double growRate,
                    int K, float* params, float* m, float* v, float* sh, float* shM, float* shV, oracle_rng_fn rng,
-                   void* ctx, ORefineOut* out) {
+                   void* ctx, ORefineOut* out, int donorSampling) {
   auto sig = [](double x) { return 1.0 / (1.0 + std::exp(-x)); };
   std::vector<uint32_t> dead, donors;
   for (uint32_t i = 0; i < n; ++i) {
@@ -307,6 +310,14 @@ void oracle_refine(uint32_t n, uint32_t cap, uint32_t growLimit, double iter, do
     const float* p = params + (size_t)i * 16;
     return ((double)p[3] + (double)p[4] + (double)p[5]) / 3.0;
   };
+  std::vector<double> cdf;
+  if (donorSampling == 1) {
+    double acc = 0.0;
+    for (uint32_t i : donors) {
+      acc += sig((double)params[(size_t)i * 16 + 13]);
+      cdf.push_back(acc);
+    }
+  }
   std::vector<uint32_t> big(donors);
   std::stable_sort(big.begin(), big.end(), [&](uint32_t a, uint32_t b) { return mls(b) - mls(a) < 0; });
   big.resize(std::min(big.size(), std::max<size_t>(16, donors.size() >> 2)));
@@ -324,8 +335,13 @@ void oracle_refine(uint32_t n, uint32_t cap, uint32_t growLimit, double iter, do
       don = big[di];
       big[di] = big.back();
       big.pop_back();
-    } else {
+    } else if (cdf.empty()) {
       don = donors[(size_t)(int32_t)(rng(ctx) * (double)donors.size())];
+    } else {
+      const double target = rng(ctx) * cdf.back();
+      size_t k = 0;
+      while (k + 1 < cdf.size() && !(cdf[k] > target)) ++k;
+      don = donors[k];
     }
     const size_t bd = (size_t)don * 16;
     const double s = std::exp(mls(don));

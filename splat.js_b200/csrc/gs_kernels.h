@@ -220,6 +220,8 @@ void launch_refine_compact(const float* params, uint32_t n, const uint32_t* dead
                            const uint32_t* donorFlag, const uint32_t* donorOff, uint32_t* deadList,
                            uint32_t* donorList, uint64_t* donorKeys, uint32_t* donorVals, cudaStream_t s);
 void launch_refine_apply(const RefineApplyArgs& a, uint32_t* splitSeq, cudaStream_t s);
+void launch_donor_opacity(const float* params, const uint32_t* donorList, uint32_t nDonors, float* out,
+                          cudaStream_t s);
 void launch_max_u32(const uint32_t* x, uint32_t count, uint32_t* out, cudaStream_t s);
 
 }  // namespace gs

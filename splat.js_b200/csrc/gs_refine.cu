@@ -11,7 +11,8 @@
 //      reference's [...donors].sort(...) (Array.prototype.sort is stable);
 //   3. the host reads three counts, draws rng() in the reference's order and
 //      uploads a plan (donor list position, split flag, three Gaussian
-//      jitters per spawn);
+//      jitters per spawn); with opacity-weighted donor sampling it also reads
+//      the donors' opacity logits (k_donor_opacity) to build the weights;
 //   4. k_refine_apply writes every spawned splat in parallel.  A donor that
 //      was split by an earlier spawn of the same call is read as the
 //      reference would see it then (log-scales shrunk by log(1/1.6)): each
@@ -126,6 +127,13 @@ __global__ void k_refine_split_donors(RefineApplyArgs a) {
   }
 }
 
+// opacity logits of the compacted donors, in donor-list order (the weights
+// of opacity-weighted donor sampling)
+__global__ void k_donor_opacity(const float* params, const uint32_t* donorList, uint32_t nDonors, float* out) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nDonors) out[k] = params[(size_t)donorList[k] * 16 + 13];
+}
+
 __global__ void k_max_u32(const uint32_t* x, uint32_t count, uint32_t* out) {
   uint32_t m = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) m = max(m, x[i]);
@@ -150,6 +158,10 @@ void launch_refine_apply(const RefineApplyArgs& a, uint32_t* splitSeq, cudaStrea
   k_refine_split_seq<<<g, 256, 0, s>>>(a.plan, a.count, a.bigSorted, splitSeq);
   k_refine_apply<<<g, 256, 0, s>>>(a);
   k_refine_split_donors<<<g, 256, 0, s>>>(a);
+}
+void launch_donor_opacity(const float* params, const uint32_t* donorList, uint32_t nDonors, float* out,
+                          cudaStream_t s) {
+  if (nDonors) k_donor_opacity<<<(nDonors + 255) / 256, 256, 0, s>>>(params, donorList, nDonors, out);
 }
 void launch_max_u32(const uint32_t* x, uint32_t count, uint32_t* out, cudaStream_t s) {
   cudaMemsetAsync(out, 0, 4, s);

@@ -236,6 +236,7 @@ int gs_default_options(gs_options* o) {
   o->useGraphs = 1;
   o->device = 0;
   o->tileCull = 1;
+  o->donorSampling = 0;
   return GS_OK;
 }
 
@@ -251,6 +252,10 @@ int gs_create(const gs_options* opts, gs_trainer** out) {
   if (!(o.eCut > 0.0f && o.eCut <= 80.0f)) { g_createError = "eCut must be in (0, 80]"; return GS_E_INVALID; }
   if (o.tile != 8 && o.tile != 16 && o.tile != 32) { g_createError = "tile must be 8, 16 or 32"; return GS_E_INVALID; }
   if (o.tileCull != 0 && o.tileCull != 1) { g_createError = "tileCull must be 0 or 1"; return GS_E_INVALID; }
+  if (o.donorSampling != 0 && o.donorSampling != 1) {
+    g_createError = "donorSampling must be 0 or 1";
+    return GS_E_INVALID;
+  }
   if (o.batchDepth != 64 && o.batchDepth != 128 && o.batchDepth != 256) {
     g_createError = "batchDepth must be 64, 128 or 256";
     return GS_E_INVALID;
@@ -1333,6 +1338,23 @@ int gs_refine(gs_trainer* h, gs_rng_fn rng, void* ctx, gs_refine_result* out) {
   ra.sweepGrid = (unsigned)h->sweepGrid;
   launch_radix_sort(ra, s);
   const uint32_t* bigSorted = h->pvals[0];  // 8 passes: result back in buffer 0
+  // opacity-weighted donor sampling: cumulative sigmoid(opacity) over the
+  // donor list (index order), in double; a clone pick is the first donor
+  // whose cumulative weight exceeds rng() * total
+  std::vector<double> cdf;
+  if (h->o.donorSampling == 1) {
+    std::vector<float> logit(nDonors);
+    float* dLogit = reinterpret_cast<float*>(h->rf.splitSeq);  // free until the plan is applied
+    launch_donor_opacity(h->params, h->rf.donorList, nDonors, dLogit, s);
+    GS_CK(cudaMemcpyAsync(logit.data(), dLogit, (size_t)nDonors * 4, cudaMemcpyDeviceToHost, s));
+    GS_CK(cudaStreamSynchronize(s));
+    cdf.resize(nDonors);
+    double acc = 0.0;
+    for (uint32_t k = 0; k < nDonors; ++k) {
+      acc += 1.0 / (1.0 + std::exp(-(double)logit[k]));
+      cdf[k] = acc;
+    }
+  }
   // the host plan: rng() draws in the reference's order
   const uint32_t moveCap = (uint32_t)std::ceil((double)n * 0.05);
   const uint32_t moved = std::min(nDead, moveCap);
@@ -1363,7 +1385,13 @@ int gs_refine(gs_trainer* h, gs_rng_fn rng, void* ctx, gs_refine_result* out) {
       big.pop_back();
       sp.split = 1;
     } else {
-      sp.pos = (uint32_t)(int32_t)(rng(ctx) * (double)nDonors);
+      const double u = rng(ctx);
+      if (cdf.empty()) {
+        sp.pos = (uint32_t)(int32_t)(u * (double)nDonors);
+      } else {
+        const size_t k = (size_t)(std::upper_bound(cdf.begin(), cdf.end(), u * cdf.back()) - cdf.begin());
+        sp.pos = (uint32_t)std::min<size_t>(k, nDonors - 1);
+      }
       sp.split = 0;
     }
     for (int k = 0; k < 3; ++k) sp.g[k] = gauss();

@@ -25,7 +25,8 @@ class GsOptions(C.Structure):
                 ("minScale", C.c_double), ("growRate", C.c_double), ("growUntil", C.c_double),
                 ("opacityReg", C.c_float), ("shLr", C.c_float), ("tile", C.c_int32), ("batchDepth", C.c_int32),
                 ("maxBatch", C.c_int32), ("backwardVariant", C.c_int32), ("persistent", C.c_int32),
-                ("useGraphs", C.c_int32), ("device", C.c_int32), ("tileCull", C.c_int32)]
+                ("useGraphs", C.c_int32), ("device", C.c_int32), ("tileCull", C.c_int32),
+                ("donorSampling", C.c_int32)]
 
 
 class GsCamera(C.Structure):

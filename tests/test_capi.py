@@ -31,7 +31,7 @@ def test_library_builds_and_exports_every_declared_symbol():
     assert not missing, missing
     # the binding covers the header exactly
     N.lib()
-    assert N.lib().gs_abi_version() == 1
+    assert N.lib().gs_abi_version() == 2
 
 
 def test_default_options_match_reference():
@@ -42,14 +42,42 @@ def test_default_options_match_reference():
     assert o.shDeg == 2 and o.tileGrad == 1 and o.capMult == 4.0 and o.maxIters == 60000
     assert o.minScale == pytest.approx(1e-4) and o.opacityReg == pytest.approx(0.01)
     assert o.shLr == pytest.approx(1.25e-4) and o.growRate == pytest.approx(0.15)
-    assert o.tile == 16 and o.tileCull == 1
+    assert o.tile == 16 and o.tileCull == 1 and o.donorSampling == 0
 
 
 def test_struct_sizes_match_header():
-    assert C.sizeof(N.GsOptions) == 4 * 6 + 8 + 4 * 2 + 8 * 4 + 4 * 2 + 4 * 8
+    assert C.sizeof(N.GsOptions) == 4 * 6 + 8 + 4 * 2 + 8 * 4 + 4 * 2 + 4 * 9 + 4  # tail padding to 8
     assert C.sizeof(N.GsCamera) == 4 * (9 + 3 + 3 + 3) + 8 * 2
     assert C.sizeof(N.GsImage) == 16
     assert C.sizeof(N.GsRefineResult) == 24
+
+
+def test_struct_layouts_match_the_c_compiler(tmp_path):
+    """Every field offset and struct size of the ctypes mirror equals what a
+    C compiler lays out from include/splat_b200.h."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    structs = {"gs_options": N.GsOptions, "gs_camera": N.GsCamera, "gs_image": N.GsImage,
+               "gs_state": N.GsState, "gs_refine_result": N.GsRefineResult, "gs_frame": N.GsFrame}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "splat_b200.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')
+        for f in py._fields_:
+            lines.append(f'  printf("{cname}.{f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(ln.split() for ln in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                   text=True).stdout.splitlines())
+    for cname, py in structs.items():
+        assert int(got[cname]) == C.sizeof(py), cname
+        for f in py._fields_:
+            assert int(got[f"{cname}.{f[0]}"]) == getattr(py, f[0]).offset, f"{cname}.{f[0]}"
 
 
 def test_create_without_device_fails_cleanly():

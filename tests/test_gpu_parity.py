@@ -317,8 +317,10 @@ def test_render_view_matches_oracle_forward():
     assert_bits(img.reshape(-1), r["img"], "renderView image")
 
 
-def test_refine_matches_oracle():
-    """Device refine vs the restated JavaScript refine with the same rng draws."""
+@pytest.mark.parametrize("donorSampling", [0, 1])
+def test_refine_matches_oracle(donorSampling):
+    """Device refine vs the restated JavaScript refine with the same rng draws
+    (donorSampling 1: the opacity-weighted donor option)."""
     n = 4000
     params, sh = scene.uniform_scene(n, seed=7, sh_deg=2)
     P = params.reshape(-1, 16)
@@ -328,7 +330,8 @@ def test_refine_matches_oracle():
     R, tt = scene.look_at_pose([0.0, 0.0, -3.0], [0.0, 0.0, 0.0])
     cams = [dict(R=R, t=tt, f=150.0, cx=64.0, cy=64.0, w=128, h=128)]
     rgbs = [scene.uniform_target(128, 128)]
-    t, targets, metas = make(params, sh, cams, rgbs, dict(shDeg=2, maxSplats=8000), radius=1.0)
+    t, targets, metas = make(params, sh, cams, rgbs, dict(shDeg=2, maxSplats=8000, donorSampling=donorSampling),
+                             radius=1.0)
     t.iter = 2000
     t.stepBatch([0])
     g = t.readGaussians()
@@ -341,7 +344,8 @@ def test_refine_matches_oracle():
     osh = np.zeros(cap * 3 * K, np.float32); osh[:n * 3 * K] = g["sh"]
     osm = np.zeros(cap * 3 * K, np.float32); osm[:n * 3 * K] = sm
     osv = np.zeros(cap * 3 * K, np.float32); osv[:n * 3 * K] = sv
-    r_cpu = O.refine(n, cap, op, om, ov, osh, osm, osv, K, rigs.lcg(31337), t.iter, 0.75 * 60000)
+    r_cpu = O.refine(n, cap, op, om, ov, osh, osm, osv, K, rigs.lcg(31337), t.iter, 0.75 * 60000,
+                     donorSampling=donorSampling)
     r_gpu = t.refine(rigs.lcg(31337))
     assert r_gpu["moved"] == r_cpu["moved"] and r_gpu["grown"] == r_cpu["grown"] and r_gpu["n"] == r_cpu["n"]
     n2 = r_gpu["n"]
