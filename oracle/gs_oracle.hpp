@@ -595,12 +595,18 @@ struct AccFixed {
     gradCam[idx] += q;
   }
 };
-// FP64 path: unquantised double sums; loss kept as a double.
+// FP64 path: unquantised double sums; loss kept as a double.  quantise
+// truncates each per-pixel contribution to the fixed-point quantum as the
+// reference does (i32(clamp(v * 16384, +-1e9)), shaders.js:529-541), in
+// double: it separates the reference's quantisation error from FP32
+// rounding when the FP32 path is compared with FP64.
 struct AccF64 {
   double* gradP;      // n * 16
   double* lossSum;    // [0] sum of Charbonnier loss, [1] sum of squared error, [2] valid px
   double* gradCam;    // (ncams + 1) * 8
+  bool quantise = false;
   void add(uint32_t id, int slot, double v) {
+    if (quantise) v = std::trunc(std::fmin(std::fmax(v * (double)FIXED, -1.0e9), 1.0e9)) / (double)FIXED;
 #pragma omp atomic
     gradP[(size_t)id * STRIDE + slot] += v;
   }

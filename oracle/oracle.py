@@ -87,7 +87,8 @@ def lib():
         L.oracle_step_f32.restype = C.c_int
         L.oracle_step_f32.argtypes = [P(OOpts), P(OCam), C.c_int, P(OAdam), C.c_uint32, f32p, f32p, u32p, f32p,
                                       f32p, f32p, f32p, u32p, i32p, f32p, f32p, C.c_int, C.c_int, u64p, f32p]
-        L.oracle_eval_f64.argtypes = [P(OOpts), P(OCam), f64p, f64p, C.c_uint32, u32p, f64p, f64p, f64p, f32p]
+        L.oracle_eval_f64.argtypes = [P(OOpts), P(OCam), f64p, f64p, C.c_uint32, u32p, f64p, f64p, f64p, f32p,
+                                      C.c_int]
         L.oracle_refine.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double,
                                     C.c_int, f32p, f32p, f32p, f32p, f32p, f32p, RNG_FN, C.c_void_p,
                                     P(ORefineOut), C.c_int]
@@ -220,8 +221,10 @@ def step(o, cams, hp, params, sh, targets, m, v, shM, shV, n, stats=None, gradCa
                 img=img)
 
 
-def eval_f64(o, c, params64, sh64, n, targets, grads=True, want_image=False):
-    """FP64 host evaluation: (loss, sqerr, validPx), gradF, shGrad (unquantised)."""
+def eval_f64(o, c, params64, sh64, n, targets, grads=True, want_image=False, quantise=False):
+    """FP64 host evaluation: (loss, sqerr, validPx), gradF, shGrad.  Unquantised
+    unless `quantise`, which truncates each per-pixel gradient contribution to
+    the reference's 1/16384 fixed-point quantum (in double)."""
     K = sh_rest(o.shDeg)
     loss3 = np.zeros(3, np.float64)
     gF = np.zeros(n * 16, np.float64) if grads else None
@@ -229,7 +232,7 @@ def eval_f64(o, c, params64, sh64, n, targets, grads=True, want_image=False):
     img = np.zeros(c.w * c.h * 4, np.float32) if want_image else None
     lib().oracle_eval_f64(C.byref(o), C.byref(c), _p(params64, C.c_double), _p(sh64, C.c_double), n,
                           _p(targets, C.c_uint32), _p(loss3, C.c_double), _p(gF, C.c_double),
-                          _p(sG, C.c_double), _p(img, C.c_float))
+                          _p(sG, C.c_double), _p(img, C.c_float), int(quantise))
     return loss3, gF, (sG[: n * 3 * K] if grads else None), img
 
 

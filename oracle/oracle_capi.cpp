@@ -258,7 +258,8 @@ int oracle_step_f32(const OOpts* oo, const OCam* cams, int V, const OAdam* oa, u
 // px) and unquantised gradients of one view.  gradF/shGrad may be null
 // (loss only, for finite differences). ----
 void oracle_eval_f64(const OOpts* oo, const OCam* oc, const double* params, const double* sh, uint32_t n,
-                     const uint32_t* targets, double* loss3, double* gradF, double* shGrad, float* outImg) {
+                     const uint32_t* targets, double* loss3, double* gradF, double* shGrad, float* outImg,
+                     int quantise) {
   const Opts o = toOpts(oo);
   const Cam c = toCam(oc);
   const int K = shRestCoefs(o.shDeg);
@@ -267,7 +268,7 @@ void oracle_eval_f64(const OOpts* oo, const OCam* oc, const double* params, cons
   Bins b = binTiles<double>(o, c, proj.data(), n);
   std::vector<double> gP((size_t)n * STRIDE, 0.0), gCam((size_t)(c.ncams + 1) * 8, 0.0);
   loss3[0] = loss3[1] = loss3[2] = 0.0;
-  AccF64 acc{gP.data(), loss3, gCam.data()};
+  AccF64 acc{gP.data(), loss3, gCam.data(), quantise != 0};
   renderView<double, AccF64>(o, c, proj.data(), b, targets, outImg, nullptr, acc, true, 0, nullptr);
   if (!gradF) return;
 #pragma omp parallel for schedule(static)

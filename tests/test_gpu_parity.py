@@ -533,6 +533,82 @@ def test_full_size_deg3_bitexact():
     assert_bits(g["sh"], s, "SH after a degree-3 full-size step")
 
 
+def test_config4_steps_refine_and_fp64_subset():
+    """Config 4 at full size: 2M splats at SH degree 3, a fifth of them fine,
+    four 1920x1080 ring views per batched step.  A step, an opacity-weighted
+    refine (relocation, and growth into 40k splats of headroom: splits and
+    clones), and a step on the grown model -- every parameter, moment and SH
+    coefficient against the oracle bit for bit -- then the FP32 gradients of
+    256 seeded visible splats against the FP64 host evaluation, with and
+    without the reference's fixed-point truncation."""
+    n, extra = 2_000_000, 40_000
+    cap = n + extra
+    K = 15
+    params, sh = scene.surface_scene(n, seed=4, sh_deg=3, log_scale=(-5.0, 0.7), fine_frac=0.2)
+    ring = scene.ring_cameras(24, 4.0, 0.5, 1920, 1080)
+    cams = [ring[k] for k in (0, 6, 12, 18)]
+    rgbs = [scene.uniform_target(1920, 1080, seed=20 + k) for k in range(4)]
+    opts = dict(shDeg=3, maxSplats=cap, batchDepth=256, entriesCap=24 * cap, donorSampling=1)
+    t, targets, metas = make(params, sh, cams, rgbs, opts, radius=4.0)
+    assert t.cap == cap
+    t.iter = 3000  # every SH band active
+    o = oracle_opts(opts)
+    ocams = [oracle_cam(metas[v], v, 4, 3) for v in range(4)]
+    P = np.zeros(cap * 16, np.float32)
+    P[:n * 16] = params
+    S = np.zeros(cap * 3 * K, np.float32)
+    S[:n * 3 * K] = sh
+    M, V = np.zeros(cap * 16, np.float32), np.zeros(cap * 16, np.float32)
+    SM, SV = np.zeros(cap * 3 * K, np.float32), np.zeros(cap * 3 * K, np.float32)
+
+    def compare(nn, what):
+        g = t.readGaussians()
+        m, v, sm, sv = t.readMoments()
+        assert g["n"] == nn
+        assert_bits(g["data"], P[:nn * 16], f"params {what}")
+        assert_bits(g["sh"], S[:nn * 3 * K], f"SH {what}")
+        assert_bits(m, M[:nn * 16], f"m {what}")
+        assert_bits(v, V[:nn * 16], f"v {what}")
+        assert_bits(sm, SM[:nn * 3 * K], f"SH m {what}")
+        assert_bits(sv, SV[:nn * 3 * K], f"SH v {what}")
+
+    t.stepBatch([0, 1, 2, 3])
+    O.step(o, ocams, oracle_adam(t, 3001, 4.0), P, S, targets, M, V, SM, SV, n)
+    compare(n, "after a 4-view step")
+    r_gpu = t.refine(rigs.lcg(2024))
+    r_cpu = O.refine(n, cap, P, M, V, S, SM, SV, K, rigs.lcg(2024), t.iter, 0.75 * 60000, donorSampling=1)
+    assert (r_gpu["moved"], r_gpu["grown"], r_gpu["n"]) == (r_cpu["moved"], r_cpu["grown"], r_cpu["n"])
+    assert r_gpu["grown"] == extra and r_gpu["moved"] > 0
+    n2 = r_gpu["n"]
+    compare(n2, "after refine")
+    t.stepBatch([0, 1, 2, 3])
+    O.step(o, ocams, oracle_adam(t, 3002, 4.0), P, S, targets, M, V, SM, SV, n2)
+    compare(n2, "after a step on the grown model")
+    # FP32 (fixed-point) gradients of one view against FP64 on 256 seeded
+    # splats that the view reaches.  The reference truncates each pixel's
+    # contribution to 1/16384 before summing (shaders.js:529-541); at 2M
+    # splats the per-splat gradients are small enough that this alone puts
+    # them a few percent (norm-wise) from exact FP64.  The FP64 evaluation
+    # with the same truncation isolates FP32 rounding, which stays small.
+    gF, sG, _ = t.gradPass(0)
+    p64, s64in = P[:n2 * 16].astype(np.float64), S[:n2 * 3 * K].astype(np.float64)
+    _, g64, s64, _ = O.eval_f64(o, ocams[0], p64, s64in, n2, targets)
+    _, g64q, s64q, _ = O.eval_f64(o, ocams[0], p64, s64in, n2, targets, quantise=True)
+    g32 = gF.reshape(-1, 16)[:, :14]
+    seen = np.flatnonzero(np.abs(g64.reshape(-1, 16)[:, :14]).sum(1) > 0)
+    pick = np.random.default_rng(256).choice(seen, 256, replace=False)
+
+    def rel(a, b, w):
+        a, b = a.reshape(-1, w)[pick], b.reshape(-1, w)[pick]
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    e_q, e_x = rel(g32, g64q.reshape(-1, 16)[:, :14], 14), rel(g32, g64.reshape(-1, 16)[:, :14], 14)
+    e_qs, e_xs = rel(sG, s64q, 3 * K), rel(sG, s64, 3 * K)
+    print(f"config 4, 256 splats, norm-wise: FP32 vs FP64 params {e_x:.3e} SH {e_xs:.3e}; "
+          f"vs FP64 with the reference's truncation params {e_q:.3e} SH {e_qs:.3e}")
+    assert e_q < 2e-3 and e_qs < 2e-3, (e_q, e_qs)
+    assert e_x < 0.1 and e_xs < 0.01, (e_x, e_xs)
+
+
 def test_lookback_timeout_is_reported_and_device_stays_usable():
     """A sort pass whose look-back can never complete gives up after a bounded
     number of spins, sets the timeout bit, and leaves the device usable."""

@@ -152,3 +152,19 @@ def test_fp32_gradients_track_fp64():
     assert rel < 5e-3, rel
     rel_sh = np.linalg.norm(sG - s64) / np.linalg.norm(s64)
     assert rel_sh < 5e-3, rel_sh
+
+
+def test_fp32_gradients_track_quantised_fp64():
+    """With the reference's per-pixel truncation applied in double as well,
+    the FP64 evaluation leaves only FP32 rounding between the two paths: the
+    ~1e-3 gap above is the fixed-point quantisation, not FP32 arithmetic."""
+    o, c, params, sh, targets, n = rig(3, True)
+    gF, sG = fp32_grads(o, c, params, sh, targets, n)
+    a = gF.reshape(-1, 16)[:, :14]
+    rel = {}
+    for q in (False, True):
+        _, g64, s64, _ = O.eval_f64(o, c, params.astype(np.float64), sh.astype(np.float64), n, targets, quantise=q)
+        b = g64.reshape(-1, 16)[:, :14]
+        rel[q] = (np.linalg.norm(a - b) / np.linalg.norm(b), np.linalg.norm(sG - s64) / np.linalg.norm(s64))
+    assert rel[True][0] < 1e-4 and rel[True][1] < 1e-4, rel
+    assert rel[True][0] < rel[False][0] / 20 and rel[True][1] < rel[False][1] / 20, rel
