@@ -89,6 +89,9 @@ def lib():
                                       f32p, f32p, f32p, u32p, i32p, f32p, f32p, C.c_int, C.c_int, u64p, f32p]
         L.oracle_eval_f64.argtypes = [P(OOpts), P(OCam), f64p, f64p, C.c_uint32, u32p, f64p, f64p, f64p, f32p,
                                       C.c_int]
+        L.oracle_fd_local_f64.argtypes = [P(OOpts), P(OCam), f64p, f64p, C.c_uint32, u32p, u32p, C.c_uint32,
+                                          f64p, C.c_uint32, f64p]
+        L.oracle_fd_local_f64.restype = C.c_int
         L.oracle_refine.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double,
                                     C.c_int, f32p, f32p, f32p, f32p, f32p, f32p, RNG_FN, C.c_void_p,
                                     P(ORefineOut), C.c_int]
@@ -234,6 +237,26 @@ def eval_f64(o, c, params64, sh64, n, targets, grads=True, want_image=False, qua
                           _p(targets, C.c_uint32), _p(loss3, C.c_double), _p(gF, C.c_double),
                           _p(sG, C.c_double), _p(img, C.c_float), int(quantise))
     return loss3, gF, (sG[: n * 3 * K] if grads else None), img
+
+
+def fd_local(o, c, params64, sh64, n, targets, ids, h=1e-4, max_tiles=1 << 20):
+    """FP64 central differences of the loss for every parameter slot (0-13)
+    and SH coefficient of the splats `ids`, over the tiles each perturbed
+    splat can touch (equal to the whole-image difference).  `h` is one step
+    or one per column.  Returns an (len(ids), 14 + 3K) array; rows of splats
+    whose tiles exceed max_tiles are NaN."""
+    K = sh_rest(o.shDeg)
+    hcol = np.ascontiguousarray(np.broadcast_to(np.asarray(h, np.float64), (14 + 3 * K,)))
+    ids = np.ascontiguousarray(ids, np.uint32)
+    out = np.zeros((len(ids), 14 + 3 * K), np.float64)
+    sh_arg = sh64 if K else np.zeros(1, np.float64)
+    rc = lib().oracle_fd_local_f64(C.byref(o), C.byref(c), _p(params64, C.c_double), _p(sh_arg, C.c_double), n,
+                                   _p(targets, C.c_uint32), _p(ids, C.c_uint32), len(ids), _p(hcol, C.c_double),
+                                   int(max_tiles),
+                                   _p(out, C.c_double))
+    if rc != 0:
+        raise RuntimeError("fd_local: the entry budget dropped a tile")
+    return out
 
 
 def refine(n, cap, params, m, v, sh, shM, shV, K, rng, iter_, growUntil, growRate=0.15, growLimit=0,

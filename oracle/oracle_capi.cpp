@@ -4,6 +4,7 @@
 // product never links it.  Layouts follow the reference: params stride 16
 // (shaders.js:14-16), SH channel-major 3K per splat (shaders.js:17-22),
 // proj stride 16 (shaders.js:23-25), gradP stride 16 i32 (shaders.js:26-28).
+#include <algorithm>
 #include <cstdio>
 #include <memory>
 
@@ -281,6 +282,140 @@ void oracle_eval_f64(const OOpts* oo, const OCam* oc, const double* params, cons
                      K ? sh + (size_t)i * 3 * K : nullptr, K, gp, gradF + (size_t)i * STRIDE,
                      (K && shGrad) ? shGrad + (size_t)i * 3 * K : shDummy, camAdd);
   }
+}
+
+// ---- FP64 central differences local to one splat's tiles ----
+// gradcheck.js:307-329 differentiates the whole-image loss.  A splat's
+// parameters change only the pixels of the tiles whose lists hold it, so in
+// L(+h) - L(-h) the loss over every other tile cancels exactly; summing the
+// union of the splat's tiles at p, p + h and p - h gives the same central
+// difference at a cost that does not grow with the image.  The perturbed
+// splat leaves each list and re-enters it where binTiles would place it
+// (rectangle, tile cull, ascending (depth bits, id)).  out: nids rows of
+// 14 parameter slots then 3K SH coefficients, column k differenced with step
+// hcol[k]; a splat whose union exceeds maxTiles gets NaN rows.  Returns -1
+// when the entry budget drops a tile.
+namespace {
+struct LocalTiles {
+  const Opts& o;
+  const Cam& c;
+  const double* proj;
+  const Bins& b;
+  const uint32_t* targets;
+  // loss over `tiles` with splat s at projection prS (prS[11] <= 0: culled)
+  double loss(const std::vector<int>& tiles, uint32_t s, const double* prS, std::vector<uint32_t>& list) const {
+    const int tile = o.tile, tx = tilesX(c, tile);
+    const bool vis = prS[11] > 0.0;
+    TileRect r{0, -1, 0, -1};
+    bool test = false;
+    CullParams cp{INFINITY, 0.0f, 0.0f};
+    float cmx = 0.0f, cmy = 0.0f;
+    if (vis) {
+      r = tileRect<double>(c, tile, prS[0], prS[1], prS[15]);
+      test = o.tileCull && !(r.x0 == r.x1 && r.y0 == r.y1);
+      if (test) {
+        const Splat2D<double> s2 = splat2D<double>(prS);
+        cmx = (float)s2.mx; cmy = (float)s2.my;
+        cp = cullParams(cmx, cmy, (float)(0.5 * s2.cA), (float)s2.cB, (float)(0.5 * s2.cC), (float)s2.w, o.aMin,
+                        o.eCut, r.x0, r.x1, r.y0, r.y1, tile);
+      }
+    }
+    const uint32_t key = fbits((float)prS[2]);
+    double lossSum[3] = {0.0, 0.0, 0.0};
+    std::vector<double> camDummy((size_t)(c.ncams + 1) * 8, 0.0);
+    AccF64 acc{nullptr, lossSum, camDummy.data(), false};
+    for (int t : tiles) {
+      const int x = t % tx, y = t / tx;
+      const bool member = vis && x >= r.x0 && x <= r.x1 && y >= r.y0 && y <= r.y1 &&
+                          (!test || tileLive(cp, cmx, cmy, x, y, tile, c.W, c.H));
+      list.clear();
+      bool placed = !member;
+      for (uint32_t k = b.start[t]; k < b.start[t + 1]; ++k) {
+        const uint32_t id = b.ids[k];
+        if (id == s) continue;
+        if (!placed && (key < b.keys[k] || (key == b.keys[k] && s < id))) { list.push_back(s); placed = true; }
+        list.push_back(id);
+      }
+      if (!placed) list.push_back(s);
+      const int ox = x * tile, oy = y * tile;
+      for (int ly = 0; ly < tile; ++ly)
+        for (int lx = 0; lx < tile; ++lx) {
+          const int gx = ox + lx, gy = oy + ly;
+          if (gx >= c.W || gy >= c.H) continue;
+          const double px = gx + 0.5, py = gy + 0.5;
+          double Tr = 1.0, C[3] = {0.0, 0.0, 0.0};
+          for (uint32_t id : list) {  // the forward of renderView, in double
+            const Splat2D<double> sp = splat2D<double>(id == s ? prS : proj + (size_t)id * STRIDE);
+            const double dx = px - sp.mx, dy = py - sp.my;
+            const double e = pairExponent(sp, dx, dy);
+            if (e > (double)o.eCut) continue;
+            const double alpha = std::fmin(0.99, sp.w * Math<double>::exp(-e));
+            if (alpha < (double)o.aMin) continue;
+            const double ta = Tr * alpha;
+            C[0] = std::fma(ta, sp.r, C[0]);
+            C[1] = std::fma(ta, sp.g, C[1]);
+            C[2] = std::fma(ta, sp.b, C[2]);
+            Tr = Tr * (1.0 - alpha);
+            if (Tr < 1e-4) break;
+          }
+          double Cf[3], gC[3];
+          for (int j = 0; j < 3; ++j) Cf[j] = C[j] + Tr * (double)c.bg[j];
+          lossPixel<double>(c, targets, (uint32_t)(gy * c.W + gx), Cf, gC, acc);
+        }
+    }
+    return lossSum[0];
+  }
+};
+}  // namespace
+
+int oracle_fd_local_f64(const OOpts* oo, const OCam* oc, const double* params, const double* sh, uint32_t n,
+                        const uint32_t* targets, const uint32_t* ids, uint32_t nids, const double* hcol,
+                        uint32_t maxTiles, double* out) {
+  const Opts o = toOpts(oo);
+  const Cam c = toCam(oc);
+  const int K = shRestCoefs(o.shDeg);
+  const int np = 14 + 3 * K;
+  std::vector<double> proj((size_t)n * STRIDE);
+  oracle_project_f64(oo, oc, params, sh, n, proj.data());
+  const Bins b = binTiles<double>(o, c, proj.data(), n);
+  if (b.overflowTiles) return -1;
+  const LocalTiles lt{o, c, proj.data(), b, targets};
+  const int tx = tilesX(c, o.tile);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long q = 0; q < (long)nids; ++q) {
+    const uint32_t s = ids[q];
+    double P[STRIDE], prp[STRIDE], prm[STRIDE];
+    std::vector<double> S((size_t)std::max(1, 3 * K), 0.0);
+    std::memcpy(P, params + (size_t)s * STRIDE, sizeof(P));
+    if (K) std::memcpy(S.data(), sh + (size_t)s * 3 * K, sizeof(double) * 3 * K);
+    std::vector<int> tiles;
+    std::vector<uint32_t> list;
+    auto addRect = [&](const double* pr) {
+      if (!(pr[11] > 0.0)) return;
+      const TileRect r = tileRect<double>(c, o.tile, pr[0], pr[1], pr[15]);
+      for (int y = r.y0; y <= r.y1; ++y)
+        for (int x = r.x0; x <= r.x1; ++x) tiles.push_back(y * tx + x);
+    };
+    for (int k = 0; k < np; ++k) {
+      double* v = k < 14 ? &P[k] : &S[(size_t)(k - 14)];
+      const double v0 = *v, h = hcol[k];
+      *v = v0 + h;
+      projectOne<double>(o, c, P, K ? S.data() : nullptr, K, prp);
+      *v = v0 - h;
+      projectOne<double>(o, c, P, K ? S.data() : nullptr, K, prm);
+      *v = v0;
+      tiles.clear();
+      addRect(proj.data() + (size_t)s * STRIDE);
+      addRect(prp);
+      addRect(prm);
+      std::sort(tiles.begin(), tiles.end());
+      tiles.erase(std::unique(tiles.begin(), tiles.end()), tiles.end());
+      double& o_ = out[(size_t)q * np + k];
+      if (tiles.size() > maxTiles) { o_ = NAN; continue; }
+      o_ = (lt.loss(tiles, s, prp, list) - lt.loss(tiles, s, prm, list)) / (2.0 * h);
+    }
+  }
+  return 0;
 }
 
 // ---- refine: MCMC-lite relocation + growth (trainer.js:666-794) ----

@@ -168,3 +168,34 @@ def test_fp32_gradients_track_quantised_fp64():
         rel[q] = (np.linalg.norm(a - b) / np.linalg.norm(b), np.linalg.norm(sG - s64) / np.linalg.norm(s64))
     assert rel[True][0] < 1e-4 and rel[True][1] < 1e-4, rel
     assert rel[True][0] < rel[False][0] / 20 and rel[True][1] < rel[False][1] / 20, rel
+
+
+@pytest.mark.parametrize("cull", [0, 1])
+def test_local_central_differences_equal_whole_image_ones(cull):
+    """fd_local (the loss over the tiles a perturbed splat can touch) equals
+    the whole-image central difference: the other tiles cancel."""
+    o, c, params, sh, targets, n = rig(3, True)
+    o.tileCull = cull
+    p64, s64 = params.astype(np.float64), sh.astype(np.float64)
+    K = O.sh_rest(3)
+    ids = [3, 41, 77, 150]
+    h = 1e-4
+    fd = O.fd_local(o, c, p64, s64, n, targets, ids, h=h)
+    rnd = rigs.lcg(5)
+    checked = 0
+    for r, s in enumerate(ids):
+        for k in [0, 1, 2, 3, 5, 6, 8, 10, 12, 13] + [14 + int(rnd() * 3 * K) for _ in range(3)]:
+            arr, j = (p64, s * 16 + k) if k < 14 else (s64, s * 3 * K + k - 14)
+            orig = arr[j]
+            arr[j] = orig + h
+            lp = O.eval_f64(o, c, p64, s64, n, targets, grads=False)[0][0]
+            arr[j] = orig - h
+            lm = O.eval_f64(o, c, p64, s64, n, targets, grads=False)[0][0]
+            arr[j] = orig
+            whole = (lp - lm) / (2 * h)
+            # the whole-image loss (~4e3) is summed in a thread-dependent
+            # order: ~1e-12 per sum, ~1e-8 in the difference quotient
+            assert abs(fd[r, k] - whole) <= 1e-6, (s, k, fd[r, k], whole)
+            checked += 1
+    assert checked == 4 * 13
+    assert np.isfinite(fd).all() and (np.abs(fd) > 0).sum() > fd.size // 2
