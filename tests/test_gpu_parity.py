@@ -533,6 +533,77 @@ def test_full_size_deg3_bitexact():
     assert_bits(g["sh"], s, "SH after a degree-3 full-size step")
 
 
+def config1_trainer(params, sh, cams, images, seed):
+    t = GSTrainer.create(dict(shDeg=2, maxSplats=len(params) // 16))
+    t.setup(dict(data=params, n=len(params) // 16, sh=sh), cams, images, 1280, 720, 4.0)
+    t.iter = 2000          # all SH bands active
+    t.rand = rigs.lcg(seed)
+    return t
+
+
+def test_config1_plain_steps():
+    """Config 1 at full size: the 500k-splat surface scene at SH degree 2, 12
+    ring cameras at 1280x720, targets rendered from a perturbed copy (N(0,
+    0.02) on every parameter).  Plain steps with the reference's rand()
+    camera pick (stepOnce): the first three bit-exact against the oracle --
+    parameters, SH, Adam moments, stats -- then 200 consecutive steps that are
+    bitwise identical across two runs and lower the loss."""
+    n, K = 500_000, 8
+    params, sh = scene.surface_scene(n, seed=1, sh_deg=2, log_scale=(-5.0, 0.7))
+    cams = scene.ring_cameras(12, 4.0, 0.5, 1280, 720)
+    for k, c in enumerate(cams):
+        c["imgIdx"] = k
+    pp, ps = scene.perturb(params, sh, 0.02, seed=2)
+    blank = [dict(tw=1280, th=720, rgb=np.zeros(1280 * 720 * 3, np.float32)) for _ in cams]
+    r = GSTrainer.create(dict(shDeg=2, maxSplats=n))
+    r.setup(dict(data=pp, n=n, sh=ps), cams, blank, 1280, 720, 4.0)
+    images = [dict(tw=1280, th=720, rgb=np.ascontiguousarray(np.clip(r.renderView(c)[..., :3], 0, 1).reshape(-1)))
+              for c in cams]
+    del r
+    targets, metas = scene.pack_targets(images, cams)
+    t = config1_trainer(params, sh, cams, images, seed=77)
+    o = oracle_opts(dict(shDeg=2))
+    p, s = params.copy(), sh.copy()
+    m, v = np.zeros(n * 16, np.float32), np.zeros(n * 16, np.float32)
+    sm, sv = np.zeros(n * 3 * K, np.float32), np.zeros(n * 3 * K, np.float32)
+    stats = np.zeros(4, np.uint32)
+    for k in range(3):
+        t.stepOnce()
+        ci = t.lastCam
+        O.step(o, [oracle_cam(metas[ci], ci, 12, 2)], oracle_adam(t, 2001 + k, 4.0), p, s, targets, m, v, sm, sv,
+               n, stats=stats)
+    g = t.readGaussians()
+    gm, gv, gsm, gsv = t.readMoments()
+    assert_bits(g["data"], p, "params after 3 plain steps")
+    assert_bits(g["sh"], s, "SH after 3 plain steps")
+    assert_bits(gm, m, "Adam m")
+    assert_bits(gv, v, "Adam v")
+    assert_bits(gsm, sm, "SH-Adam m")
+    assert_bits(gsv, sv, "SH-Adam v")
+    first = t.readLoss()
+    assert first == stats[0] / 16 / (stats[2] * 3)
+    # 200 consecutive steps, twice
+    runs = []
+    for rep in range(2):
+        u = t if rep == 0 else config1_trainer(params, sh, cams, images, seed=77)
+        if rep == 1:
+            for _ in range(3):
+                u.stepOnce()
+            u.readLoss()
+        losses = []
+        for k in range(197):
+            u.stepOnce()
+            if k % 12 == 11:
+                losses.append(u.readLoss())
+        g = u.readGaussians()
+        runs.append((g["data"], g["sh"], losses))
+    assert_bits(runs[1][0], runs[0][0], "params after 200 steps, second run")
+    assert_bits(runs[1][1], runs[0][1], "SH after 200 steps, second run")
+    losses = runs[0][2]
+    print(f"config 1 loss (MSE per channel): after 3 steps {first:.6f}, over the last 12 steps {losses[-1]:.6f}")
+    assert losses[-1] < first, (first, losses)
+
+
 def gradcheck_relerr(a, b, floor=1e-3):
     """gradcheck.js's per-element measure: |a - b| / max(|a|, |b|), 0 where
     both are below `floor`."""
