@@ -4,7 +4,8 @@ A fake library stands in for libsplat_b200.so, so these run on the CPU.
 They cover the parts the reference keeps on the host: the rand() camera
 pick with the holdout/excluded skip (trainer.js:400-406), the camera-pose
 Adam of _applyCamGrads (trainer.js:476-537) with its every-25-iterations
-trigger (trainer.js:467-469), and readLoss (trainer.js:615-631).  Each is
+trigger (trainer.js:467-469), readLoss (trainer.js:615-631), and the eval
+passes' PSNR and test-time pose refinement (trainer.js:542-612).  Each is
 checked against a statement-for-statement transcription of the
 JavaScript."""
 import copy
@@ -224,3 +225,102 @@ def test_read_loss_follows_the_reference(monkeypatch):
     fake.pixels = 10
     fake.stats = [5, 0, 0, 0]
     assert t.readLoss() is None                  # no valid pixel
+
+
+def pose_response(R, t, g, b, nr, ci):
+    """A smooth stand-in for the device: stats and camera gradients as
+    functions of the pose the pass renders (float32 R and t, as the camera
+    record carries them)."""
+    R = np.asarray(R, np.float32).astype(np.float64)
+    t = np.asarray(t, np.float32).astype(np.float64)
+    cg = np.zeros(nr * 8, np.int64)
+    for k in range(8):
+        cg[ci * 8 + k] = int(round(3000 * math.sin(1.3 * k + R[k % 9] + 2 * t[k % 3] + 3 * g + 5 * b)))
+    v = int(4e6 * (1.5 + math.sin(R.sum() + t.sum() + g - b)))
+    return [v, 0, 5000, 0], cg
+
+
+class EvalLib(FakeLib):
+    def __init__(self, metas):
+        super().__init__()
+        self.metas = metas
+        self.seen = []
+
+    def gs_eval_pass(self, h, ci, cam, st, cgp):
+        if cam is None:
+            m = self.metas[ci]
+            R, t, g, b = m["R"], m["t"], m["g"], m["b"]
+        else:
+            s = cam._obj
+            R, t, g, b = list(s.R), list(s.t), s.g, s.b
+        self.seen.append((list(np.float32(R)), list(np.float32(t)), g, b))
+        stats, cg = pose_response(R, t, g, b, len(self.metas) + 1, ci)
+        for k in range(4):
+            st[k] = stats[k]
+        for k, x in enumerate(cg):
+            cgp[k] = int(x)
+        return 0
+
+
+def js_psnr(stats):
+    """_evalPass (trainer.js:564-572)."""
+    mse = stats[0] / 16 / (max(1, stats[2]) * 3)
+    return -10 * math.log10(mse) if mse > 0 else math.inf
+
+
+def js_eval_refined(meta, ci, nr, steps, radius, expComp):
+    """evalCamPsnrRefined (trainer.js:584-612) against pose_response."""
+    R, t, g, b = list(meta["R"]), list(meta["t"]), 0.0, 0.0
+    m, v = [0.0] * 8, [0.0] * 8
+    b1, b2, eps = 0.9, 0.99, 1e-15
+    rotLr, trnLr, expLr = 3e-4, 3e-4 * radius, 5e-3
+    for s in range(1, steps + 1):
+        _, cg = pose_response(R, t, g, b, nr, ci)
+        upd = [0.0] * 8
+        for k in range(8):
+            grad = cg[ci * 8 + k] / 64
+            m[k] = b1 * m[k] + (1 - b1) * grad
+            v[k] = b2 * v[k] + (1 - b2) * grad * grad
+            mh = m[k] / (1 - math.pow(b1, s))
+            vh = v[k] / (1 - math.pow(b2, s))
+            upd[k] = (rotLr if k < 3 else (trnLr if k < 6 else expLr)) * mh / (math.sqrt(vh) + eps)
+        R = js_m3mul(js_rodrigues([-upd[0], -upd[1], -upd[2]]), R)
+        t = [t[0] - upd[3], t[1] - upd[4], t[2] - upd[5]]
+        if expComp:
+            g = max(-0.1, min(0.1, g - upd[6]))
+            b = max(-0.05, min(0.05, b - upd[7]))
+    stats, _ = pose_response(R, t, g, b, nr, ci)
+    return js_psnr(stats), (R, t, g, b)
+
+
+def test_eval_psnr_follows_the_reference(monkeypatch):
+    t = bare_trainer(FakeLib(), monkeypatch, ncams=4)
+    lib = EvalLib(t.camMeta)
+    monkeypatch.setattr(N, "lib", lambda: lib)
+    for ci in range(4):
+        stats, _ = pose_response(t.camMeta[ci]["R"], t.camMeta[ci]["t"], 0.0, 0.0, 5, ci)
+        assert t.evalCamPsnr(ci) == js_psnr(stats)
+    assert js_psnr([0, 0, 0, 0]) == math.inf
+    def no_valid_pixel(h, ci, cam, st, cg):
+        for k, x in enumerate([96, 0, 0, 0]):
+            st[k] = x
+        return 0
+    lib.gs_eval_pass = no_valid_pixel
+    assert t.evalCamPsnr(1) == -10 * math.log10(96 / 16 / 3)     # validPx 0 counts as 1
+
+
+@pytest.mark.parametrize("expComp", [False, True])
+def test_eval_refined_pose_follows_the_reference(monkeypatch, expComp):
+    """Test-time pose refinement of one camera: the Adam loop over the
+    pass's camera gradients, then the PSNR at the refined pose."""
+    t = bare_trainer(FakeLib(), monkeypatch, ncams=4, opts=dict(expComp=expComp), radius=1.7)
+    lib = EvalLib(t.camMeta)
+    monkeypatch.setattr(N, "lib", lambda: lib)
+    ci, steps = 2, 30
+    got = t.evalCamPsnrRefined(ci, steps)
+    want, (R, tt, g, b) = js_eval_refined(t.camMeta[ci], ci, 5, steps, 1.7, expComp)
+    assert len(lib.seen) == steps + 1
+    assert got == want
+    last = lib.seen[-1]
+    assert last[0] == list(np.float32(R)) and last[1] == list(np.float32(tt))
+    assert (last[2], last[3]) == (g, b) and ((g, b) != (0.0, 0.0)) == expComp
