@@ -324,3 +324,27 @@ def test_eval_refined_pose_follows_the_reference(monkeypatch, expComp):
     last = lib.seen[-1]
     assert last[0] == list(np.float32(R)) and last[1] == list(np.float32(tt))
     assert (last[2], last[3]) == (g, b) and ((g, b) != (0.0, 0.0)) == expComp
+
+
+def so3_log(R):
+    """Rotation -> axis-angle (restated for the round trip below)."""
+    c = max(-1.0, min(1.0, (R[0] + R[4] + R[8] - 1) / 2))
+    th = math.acos(c)
+    if th < 1e-12:
+        return [0.0, 0.0, 0.0]
+    k = th / (2 * math.sin(th))
+    return [k * (R[7] - R[5]), k * (R[2] - R[6]), k * (R[3] - R[1])]
+
+
+def test_rodrigues_properties_of_the_reference_tests():
+    """tests/unit/test_geometry.mjs:41-49 for the mirror's rodrigues: the
+    log-map round trip within 1e-10 and det R = 1 within 1e-12; plus
+    orthonormality and the identity below 1e-12 rad."""
+    w = [0.3, -0.7, 0.2]
+    R = T.rodrigues(w)
+    assert max(abs(a - b) for a, b in zip(w, so3_log(R))) < 1e-10
+    M = np.asarray(R, np.float64).reshape(3, 3)
+    assert abs(np.linalg.det(M) - 1) < 1e-12
+    assert np.abs(M @ M.T - np.eye(3)).max() < 1e-12
+    assert T.rodrigues([1e-13, 0.0, 0.0]) == [1.0, 0, 0, 0, 1.0, 0, 0, 0, 1.0]
+    assert np.allclose(np.asarray(T.m3mul(R, T.rodrigues([-0.3, 0.7, -0.2]))).reshape(3, 3), np.eye(3), atol=1e-12)
