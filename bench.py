@@ -15,7 +15,8 @@ is several GB, larger than the 126 MB L2, so no flush is needed.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 --impl reference times the CPU restatement of the reference's step (the
-oracle, all host threads) on a bounded sample of the same workload.
+oracle, all host threads): each step one whole view of the workload
+(cameras 0-7 in turn), plus one step on a single thread.
 """
 from __future__ import annotations
 
@@ -185,60 +186,68 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU side (oracle): baseline sample and the --impl reference arm
 # ---------------------------------------------------------------------------
-def cpu_view_sample(args, params, sh, cams, targets, offsets, ci=0, tile_stride=16):
-    """One plain step of camera ci on the host: project, bin, chain and Adam in
-    full, the raster on every tile_stride-th tile, scaled to a full view."""
+CPU_CAMS = 8  # the CPU arm trains cameras 0..7 in turn: the views of the GPU arm's first batch
+
+
+def cpu_adam_hp(iter_after, radius, horizon=60000):
+    """The trainer's Adam uniforms after `iter_after` increments
+    (trainer.js:319-342, 417-424): position lr 3e-4 r decayed to 1% at 75% of
+    the horizon, scale 5e-3, rotation 1e-3, colour 1.5e-2, opacity 2.5e-2;
+    log-scale clamps [log(1e-4 r), log(0.05 r)]."""
     from oracle import oracle as O
-    n = len(params) // 16
-    K = 8
-    o = O.opts(shDeg=2, entriesCap=max(12_000_000, n * 24))
-    c = cams[ci]
-    oc = O.cam(c["R"], c["t"], c["f"], c["cx"], c["cy"], c["w"], c["h"], offset=offsets[ci], camIdx=ci,
-               ncams=len(cams), activeSh=2.0)
-    t0 = time.perf_counter()
-    proj = O.project(o, oc, params, sh, n)
-    bins = O.bin_tiles(o, oc, proj, n, cap=max(1, n * 40))
-    t1 = time.perf_counter()
-    pairs, gradP = O.render_sample(o, oc, proj, bins, targets, n, tile_stride, train=True, ncams=len(cams))
-    t2 = time.perf_counter()
-    gradCam = np.zeros((len(cams) + 1) * 8, np.int32)
-    gF, sG = O.chain(o, oc, params, proj, sh, n, gradP, gradCam)
-    m = np.zeros_like(params)
-    v = np.zeros_like(params)
-    sm = np.zeros_like(sh)
-    sv = np.zeros_like(sh)
-    hp = O.adam_hp([1e-4] * 14 + [0, 0], 2001, -9.2, -3.0)
-    O.adam(hp, n, K, params.copy(), gF, m, v, sh.copy(), sG, sm, sv)
-    t3 = time.perf_counter()
-    fixed = (t1 - t0) + (t3 - t2)
-    raster_full = (t2 - t1) * tile_stride
-    return dict(seconds=fixed + raster_full, fixed=fixed, raster_sample=t2 - t1, tile_stride=tile_stride,
-                sample_pairs=pairs)
+    pos = 3e-4 * radius * math.pow(0.01, min(1.0, iter_after / (0.75 * horizon)))
+    lr = [pos, pos, pos, 5e-3, 5e-3, 5e-3, 1e-3, 1e-3, 1e-3, 1e-3, 1.5e-2, 1.5e-2, 1.5e-2, 2.5e-2, 0, 0]
+    lr = [float(np.float32(x)) for x in lr]
+    return O.adam_hp(lr, iter_after, float(np.float32(math.log(radius * 1e-4))),
+                     float(np.float32(math.log(radius * 0.05))))
 
 
-def cpu_targets(args, params, sh, cams, tile_stride):
-    """Targets for the CPU arm (same recipe as the GPU arm: a perturbed copy
-    rendered forward), only for the sampled tiles of camera 0."""
+def cpu_setup(args, params, sh, cams, ncams):
+    """Inputs of the CPU arm: targets of cameras 0..ncams-1 rendered forward
+    by the oracle from the same perturbed copy the GPU arm renders its targets
+    from, packed RGBA8 as setup does (trainer.js:115-139)."""
     from oracle import oracle as O
     from splat_b200 import scene
     n = len(params) // 16
     pp, ps = scene.perturb(params, sh, 0.02, seed=args.seed + 1)
-    total = sum(c["w"] * c["h"] for c in cams)
-    offsets, acc = [], 0
-    for c in cams:
-        offsets.append(acc)
-        acc += c["w"] * c["h"]
-    targets = np.zeros(total, np.uint32)
     o = O.opts(shDeg=2, entriesCap=max(12_000_000, n * 24))
-    c = cams[0]
-    oc = O.cam(c["R"], c["t"], c["f"], c["cx"], c["cy"], c["w"], c["h"], activeSh=2.0, train=0)
-    proj = O.project(o, oc, pp, ps, n)
-    bins = O.bin_tiles(o, oc, proj, n, cap=max(1, n * 40))
-    img = O.render(o, oc, proj, bins, targets, n, train=False)["img"].reshape(-1, 4)
-    rgb = np.clip(img[:, :3], 0, 1)
-    q = np.minimum(255, np.floor(rgb.astype(np.float64) * 255 + 0.5)).astype(np.uint32)
-    targets[:c["w"] * c["h"]] = (255 << 24) | (q[:, 2] << 16) | (q[:, 1] << 8) | q[:, 0]
-    return targets, offsets
+    sizes = [c["w"] * c["h"] for c in cams[:ncams]]
+    offsets = [int(x) for x in np.concatenate([[0], np.cumsum(sizes)[:-1]])]
+    targets = np.zeros(sum(sizes), np.uint32)
+    for ci in range(ncams):
+        c = cams[ci]
+        oc = O.cam(c["R"], c["t"], c["f"], c["cx"], c["cy"], c["w"], c["h"], activeSh=2.0, train=0)
+        proj = O.project(o, oc, pp, ps, n)
+        bins = O.bin_tiles(o, oc, proj, n, cap=max(1, n * 40))
+        img = O.render(o, oc, proj, bins, targets, n, train=False)["img"].reshape(-1, 4)
+        q = np.minimum(255, np.floor(np.clip(img[:, :3], 0, 1).astype(np.float64) * 255 + 0.5)).astype(np.uint32)
+        targets[offsets[ci]:offsets[ci] + sizes[ci]] = (255 << 24) | (q[:, 2] << 16) | (q[:, 1] << 8) | q[:, 0]
+    ocams = [O.cam(c["R"], c["t"], c["f"], c["cx"], c["cy"], c["w"], c["h"], offset=offsets[ci], camIdx=ci,
+                   ncams=len(cams), activeSh=2.0) for ci, c in enumerate(cams[:ncams])]
+    return o, ocams, targets
+
+
+class CpuTrainer:
+    """The oracle's plain training step (project, bin, per-tile sort, raster
+    forward + loss + backward, chain, Adam + SH-Adam) over whole views, on
+    its own copy of the model, starting at iteration 2000 like the GPU arm."""
+
+    def __init__(self, o, ocams, targets, params, sh, radius=4.0):
+        self.o, self.ocams, self.targets, self.radius = o, ocams, targets, radius
+        self.p, self.s = params.copy(), sh.copy()
+        self.m, self.v = np.zeros_like(self.p), np.zeros_like(self.p)
+        self.sm, self.sv = np.zeros_like(self.s), np.zeros_like(self.s)
+        self.iter = 2000
+
+    def step(self, ci):
+        """One optimiser step on camera ci; returns its wall time in seconds."""
+        from oracle import oracle as O
+        self.iter += 1
+        hp = cpu_adam_hp(self.iter, self.radius)
+        t0 = time.perf_counter()
+        O.step(self.o, [self.ocams[ci]], hp, self.p, self.s, self.targets, self.m, self.v, self.sm, self.sv,
+               len(self.p) // 16)
+        return time.perf_counter() - t0
 
 
 def run_reference(args):
@@ -248,23 +257,31 @@ def run_reference(args):
     from oracle import oracle as O
     O.build()
     params, sh, cams = workload(args)
-    cores = os.cpu_count() or 1
-    stride = 32
-    targets, offsets = cpu_targets(args, params, sh, cams, stride)
+    ncams = min(CPU_CAMS, len(cams))
+    o, ocams, targets = cpu_setup(args, params, sh, cams, ncams)
+    cores = O.set_threads(0)
+    tr = CpuTrainer(o, ocams, targets, params, sh)
     times = []
     for k in range(args.warmup + args.steps):
-        r = cpu_view_sample(args, params, sh, cams, targets, offsets, ci=0, tile_stride=stride)
+        dt = tr.step(k % ncams)
         if k >= args.warmup:
-            times.append(r["seconds"])
+            times.append(dt)
     sec = sum(times) / max(1, len(times))
     v = 1.0 / sec
-    sample = f"each step: one {args.width}x{args.height} view of camera 0; project/bin/chain/Adam over all " \
-             f"{args.splats} splats, raster on every {stride}th tile scaled by {stride}"
+    # one more whole-view step on a single host thread, beside the all-core figure
+    O.set_threads(1)
+    one = tr.step((args.warmup + args.steps) % ncams)
+    O.set_threads(cores)
+    sample = (f"each step: one whole {args.width}x{args.height} view (cameras 0-{ncams - 1} in turn), the "
+              f"oracle's plain training step over all {args.splats} splats; {cores} threads")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "views/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded surface scene)",
-            "config": config_dict(args, {"parallelism": "host threads"}),
+            "config": config_dict(args, {"parallelism": "host threads", "views_per_step": 1,
+                                         "cameras_trained": f"0-{ncams - 1} in turn"}),
             "cpu_baseline": {"value": v, "unit": "views/s", "cores": cores, "kind": "port", "sample": sample},
+            "single_thread": {"value": 1.0 / one, "unit": "views/s", "cores": 1, "ms_per_view": one * 1e3},
+            "nproc": os.cpu_count(),
             "e2e": {"value": v, "unit": "views/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -544,15 +561,19 @@ def run_ours(args):
 
 
 def cpu_baseline_line(args, params, sh, cams):
+    """The oracle's plain step on one whole view of camera 0, all host
+    threads: one untimed step, then one timed."""
     try:
         from oracle import oracle as O
         O.build()
-        stride = 32
-        targets, offsets = cpu_targets(args, params, sh, cams, stride)
-        r = cpu_view_sample(args, params, sh, cams, targets, offsets, ci=0, tile_stride=stride)
-        return {"value": 1.0 / r["seconds"], "unit": "views/s", "cores": os.cpu_count() or 1, "kind": "port",
-                "sample": f"one {args.width}x{args.height} view: project/bin/chain/Adam over all splats, raster on "
-                          f"every {stride}th tile scaled by {stride} ({r['seconds']:.1f} s/view estimated)"}
+        o, ocams, targets = cpu_setup(args, params, sh, cams, 1)
+        cores = O.set_threads(0)
+        tr = CpuTrainer(o, ocams, targets, params, sh)
+        tr.step(0)
+        sec = tr.step(0)
+        return {"value": 1.0 / sec, "unit": "views/s", "cores": cores, "kind": "port",
+                "sample": f"one whole {args.width}x{args.height} view of camera 0 (the oracle's plain training "
+                          f"step over all splats, after one untimed step): {sec:.2f} s"}
     except Exception as e:  # the baseline is reported, never required
         return {"value": None, "unit": "views/s", "cores": os.cpu_count() or 1, "kind": "port",
                 "sample": f"failed: {e}"}

@@ -245,16 +245,22 @@ GS_API int gs_debug_targets(gs_trainer* h, uint32_t* out, uint64_t count);
  * foreign allocations), and code on a path where an allocation -- which may
  * synchronise the device -- is not allowed.
  * Stable LSD radix sort of n (key, value) pairs held in device memory, in
- * place, on key bits [0, keyBits): the sort that orders the trainer's
- * (tile id, splat id) entries, run with its scratch in statically sized
- * device arrays instead of buffers the trainer allocates, so the call
- * allocates nothing.  Every GPU that loads the library holds that scratch
- * (about 8.5 MB) until the process exits.  n above GS_STATIC_SORT_MAX
- * returns GS_E_LIMIT.
+ * place, by key: the sort that orders the trainer's (tile id, splat id)
+ * entries, run with its scratch in statically sized device arrays instead
+ * of buffers the trainer allocates, so the call allocates nothing.  Keys
+ * must be below 2^keyBits: the sort runs ceil(keyBits / 8) passes over
+ * 8-bit digits, so key bits from keyBits up to the next multiple of 8 would
+ * also order the output.  Every GPU that loads the library holds that
+ * scratch (about 8.5 MB) until the process exits.  n above
+ * GS_STATIC_SORT_MAX returns GS_E_LIMIT.
  * keys/vals: device pointers on the current device; stream may be NULL.
- * The first call on a device sets the scratch up (symbol lookup and a
- * synchronous clear), so make it before any stream capture.  The call
- * returns after the sort has finished (GS_E_DEVICE on a look-back timeout).
+ * The first call on a device sets up the launch grids (device attributes
+ * and kernel occupancy), so make it before any stream capture; every call
+ * looks the scratch's device addresses up again.  Each call copies the
+ * device status word to the host and synchronises `stream` before it
+ * returns, so it returns after the sort has finished (GS_E_DEVICE on a
+ * look-back timeout).  A CUDA error that an earlier call on the thread left
+ * pending is returned as GS_E_CUDA before any work, and stays pending.
  * The scratch is shared: calls that overlap in time race. */
 #define GS_STATIC_SORT_MAX (1u << 20)
 GS_API int gs_sort_entries_static(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t keyBits, void* stream);

@@ -62,6 +62,8 @@ def lib():
         P = C.POINTER
         f32p, f64p, u32p, i32p, u64p, u8p = (P(C.c_float), P(C.c_double), P(C.c_uint32), P(C.c_int32),
                                              P(C.c_uint64), P(C.c_uint8))
+        L.oracle_set_threads.restype = C.c_int
+        L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_exp_f32.restype = C.c_float
         L.oracle_exp_f32.argtypes = [C.c_float]
         L.oracle_log_f32.restype = C.c_float
@@ -97,6 +99,12 @@ def lib():
                                     P(ORefineOut), C.c_int]
         _lib = L
     return _lib
+
+
+def set_threads(n: int = 0) -> int:
+    """Host threads of the oracle's parallel loops (n <= 0 keeps the current
+    setting); returns the count in effect."""
+    return int(lib().oracle_set_threads(int(n)))
 
 
 def _p(a, ct):

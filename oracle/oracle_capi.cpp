@@ -8,11 +8,20 @@
 #include <cstdio>
 #include <memory>
 
+#include <omp.h>
+
 #include "gs_oracle.hpp"
 
 using namespace gso;
 
 extern "C" {
+
+// Host threads the parallel loops use (the CPU baseline is timed at one
+// thread and at all of them); returns the count now in effect.
+int oracle_set_threads(int n) {
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+}
 
 // Plain-C mirrors of gso::Opts / gso::Cam (field order is the ABI).
 struct OOpts {

@@ -13,11 +13,16 @@
 // code the arrays' names are host-side stand-ins, never device addresses:
 // only the addresses cudaGetSymbolAddress returns are passed to kernels.
 //
-// Set-up: the first call on a device resolves the arrays' addresses with
-// cudaGetSymbolAddress (with that device current) and clears the look-back
-// status words once; later calls on that device only clear the per-sort
-// histograms and counters.  The scratch is shared by every caller, so two
-// calls whose work overlaps in time (different streams or host threads) race.
+// Set-up: the first call on a device computes the launch grids (device
+// attributes and kernel occupancy) once.  Every call resolves the arrays'
+// addresses again with cudaGetSymbolAddress, with the caller's device
+// current, so a context that was torn down and made again (which reloads the
+// module and may move the arrays) never sees a stale address.  The arrays
+// start zeroed whenever the module loads (static storage), which is the state
+// the epoch-tagged look-back words need; each call clears only the per-sort
+// histograms, block counters and status word.  The scratch is shared by
+// every caller, so two calls whose work overlaps in time (different streams
+// or host threads) race.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -43,45 +48,48 @@ __device__ __align__(256) uint32_t g_ssVals[SS_MAX];
 __device__ __align__(256) unsigned long long g_ssStatus[SS_STATUS];
 __device__ __align__(256) uint32_t g_ssSmall[SS_SMALL];
 
-struct StaticScratch {
+struct StaticGrids {
   bool ready = false;
+  unsigned histGrid = 0, sweepGrid = 0;
+};
+StaticGrids g_grids[SS_MAX_DEVICES];
+std::mutex g_setupMutex;
+
+struct StaticScratch {
   uint32_t* keys = nullptr;
   uint32_t* vals = nullptr;
   uint64_t* status = nullptr;
   uint32_t* small = nullptr;
   unsigned histGrid = 0, sweepGrid = 0;
 };
-StaticScratch g_scratch[SS_MAX_DEVICES];
-std::mutex g_setupMutex;
 
 __global__ void k_ss_set_count(uint32_t* word, uint32_t n) { *word = n; }
 
-// Resolves the scratch of the current device (once per device).
-int static_scratch(int device, StaticScratch** out) {
+// The scratch addresses on the current device (looked up on every call) and
+// the launch grids (computed once per device).
+int static_scratch(int device, StaticScratch* sc) {
   if (device < 0 || device >= SS_MAX_DEVICES) return GS_E_INVALID;
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_ssKeys) != cudaSuccess) return GS_E_CUDA;
+  sc->keys = static_cast<uint32_t*>(p);
+  if (cudaGetSymbolAddress(&p, g_ssVals) != cudaSuccess) return GS_E_CUDA;
+  sc->vals = static_cast<uint32_t*>(p);
+  if (cudaGetSymbolAddress(&p, g_ssStatus) != cudaSuccess) return GS_E_CUDA;
+  sc->status = static_cast<uint64_t*>(p);
+  if (cudaGetSymbolAddress(&p, g_ssSmall) != cudaSuccess) return GS_E_CUDA;
+  sc->small = static_cast<uint32_t*>(p);
   std::lock_guard<std::mutex> lock(g_setupMutex);
-  StaticScratch& sc = g_scratch[device];
-  if (!sc.ready) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_ssKeys) != cudaSuccess) return GS_E_CUDA;
-    sc.keys = static_cast<uint32_t*>(p);
-    if (cudaGetSymbolAddress(&p, g_ssVals) != cudaSuccess) return GS_E_CUDA;
-    sc.vals = static_cast<uint32_t*>(p);
-    if (cudaGetSymbolAddress(&p, g_ssStatus) != cudaSuccess) return GS_E_CUDA;
-    sc.status = static_cast<uint64_t*>(p);
-    if (cudaGetSymbolAddress(&p, g_ssSmall) != cudaSuccess) return GS_E_CUDA;
-    sc.small = static_cast<uint32_t*>(p);
-    // status words and the epoch start at zero; synchronous, before first use
-    if (cudaMemset(sc.status, 0, sizeof(g_ssStatus)) != cudaSuccess) return GS_E_CUDA;
-    if (cudaMemset(sc.small, 0, sizeof(g_ssSmall)) != cudaSuccess) return GS_E_CUDA;
+  StaticGrids& g = g_grids[device];
+  if (!g.ready) {
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return GS_E_CUDA;
-    sc.histGrid = (unsigned)(sms * 4);
-    sc.sweepGrid = (unsigned)onesweep_grid(device);
-    if (cudaDeviceSynchronize() != cudaSuccess) return GS_E_CUDA;
-    sc.ready = true;
+    g.histGrid = (unsigned)(sms * 4);
+    g.sweepGrid = (unsigned)onesweep_grid(device);
+    if (g.sweepGrid == 0) return GS_E_CUDA;
+    g.ready = true;
   }
-  *out = &sc;
+  sc->histGrid = g.histGrid;
+  sc->sweepGrid = g.sweepGrid;
   return GS_OK;
 }
 
@@ -95,11 +103,15 @@ extern "C" int gs_sort_entries_static(uint32_t* keys, uint32_t* vals, uint32_t n
   if (keyBits < 1 || keyBits > 32) return GS_E_INVALID;
   if (n == 0) return GS_OK;
   if (!keys || !vals) return GS_E_INVALID;
+  // an error an earlier call on this thread left pending is reported, and
+  // left pending, rather than taken for a failure of this call's launches
+  if (cudaPeekAtLastError() != cudaSuccess) return GS_E_CUDA;
   int device = -1;
   if (cudaGetDevice(&device) != cudaSuccess) return GS_E_CUDA;
-  StaticScratch* sc = nullptr;
-  const int rc = static_scratch(device, &sc);
+  StaticScratch scr;
+  const int rc = static_scratch(device, &scr);
   if (rc != GS_OK) return rc;
+  StaticScratch* sc = &scr;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   uint32_t* statusWord = sc->small + SS_HIST + 8;
   uint32_t* epoch = sc->small + SS_HIST + 9;

@@ -508,6 +508,7 @@ int gs_set_camera(gs_trainer* h, uint32_t ci, const gs_camera* cam) {
   h->cams[ci] = *cam;
   h->cams[ci].w = w; h->cams[ci].h = hh; h->cams[ci].imgIdx = im;  // training resolution stays the image's
   h->camIdxZero = false;  // _applyCamGrads rebuilds every camUniform with its index (trainer.js:533)
+  h->camActiveSh[ci] = (float)h->o.shDeg;  // ... and with every SH band active (_camUniform, trainer.js:367)
   return GS_OK;
 }
 
@@ -1030,9 +1031,17 @@ int gs_eval_pass(gs_trainer* h, uint32_t ci, const gs_camera* cam, uint32_t stat
   int rc = check_views(h, &ci, 1);
   if (rc) return rc;
   cudaSetDevice(h->device);
-  gs_camera c = cam ? *cam : h->cams[ci];
+  const bool over = cam != nullptr;
+  gs_camera c = over ? *cam : h->cams[ci];
   c.w = h->cams[ci].w; c.h = h->cams[ci].h;
-  const DevCam view = make_cam(h, c, 1, h->camOffset[ci], ci, h->camActiveSh[ci]);
+  // With an override the reference builds a fresh uniform (trainer.js:547):
+  // gradient row ci and every SH band active.  Without one it reuses
+  // camUniforms[ci] as the last step or rebuild left it: the ramped SH degree
+  // of that camera's last step, and gradient row 0 after growth rebuilt the
+  // uniforms without their index (trainer.js:768).
+  const uint32_t row = (!over && h->camIdxZero) ? 0u : ci;
+  const float act = over ? (float)h->o.shDeg : h->camActiveSh[ci];
+  const DevCam view = make_cam(h, c, 1, h->camOffset[ci], row, act);
   GS_CK(cudaMemsetAsync(h->stats, 0, 16, h->stream));
   upload_params(h, &view, 1, make_hp(h));
   rc = run_shape(h, make_shape(h, &view, 1, 3, 1, 0, 0));

@@ -102,3 +102,32 @@ def test_static_sort_edge_sizes():
         o = np.argsort(keys, kind="stable")
         np.testing.assert_array_equal(dk.cpu().numpy().view(np.uint32), keys[o])
         np.testing.assert_array_equal(dv.cpu().numpy().view(np.uint32), vals[o])
+
+
+def test_static_sort_at_the_limit_allocates_nothing():
+    """A call of exactly GS_STATIC_SORT_MAX entries (3 radix passes, so the
+    result is copied back from the scratch half) sorts correctly and leaves
+    the device's free memory unchanged; one entry more is refused with
+    GS_E_LIMIT before any device work."""
+    import torch
+    L = N.lib()
+    n = N.STATIC_SORT_MAX
+    rng = np.random.default_rng(11)
+    keys = rng.integers(0, 1 << 20, n, dtype=np.uint32)
+    vals = np.arange(n, dtype=np.uint32)
+    dk = torch.from_numpy(keys.view(np.int32)).cuda()
+    dv = torch.from_numpy(vals.view(np.int32)).cuda()
+    wk, wv = dk.clone(), dv.clone()
+    torch.cuda.synchronize()
+    # warm-up call: loads the library's kernels on this device (lazy module loading)
+    assert L.gs_sort_entries_static(C.c_void_p(wk.data_ptr()), C.c_void_p(wv.data_ptr()), n, 20, None) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    rc = L.gs_sort_entries_static(C.c_void_p(dk.data_ptr()), C.c_void_p(dv.data_ptr()), n, 20, None)
+    free1, _ = torch.cuda.mem_get_info()
+    assert rc == 0, rc
+    assert free1 == free0, (free0, free1)
+    o = np.argsort(keys, kind="stable")
+    np.testing.assert_array_equal(dk.cpu().numpy().view(np.uint32), keys[o])
+    np.testing.assert_array_equal(dv.cpu().numpy().view(np.uint32), vals[o])
+    assert L.gs_sort_entries_static(C.c_void_p(dk.data_ptr()), C.c_void_p(dv.data_ptr()), n + 1, 20, None) == -5
