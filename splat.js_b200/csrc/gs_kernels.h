@@ -23,6 +23,7 @@ struct ProjectArgs {
   int32_t* diffGrid;       // per view (tilesX+1)*(tilesY+1), cleared before
   const uint32_t* gridBase;  // V offsets into diffGrid
   float4* cullRecs;        // V * n warp-block cull parameters (p, q, kA, 0)
+  uint4* itemSrc;          // V * n * 2: per visible slot (rect, mean, cull parameters, slot) for the expansion
 };
 
 struct TileRangeArgs {
@@ -46,10 +47,9 @@ struct ExpandArgs {
   int V;
   const DevCam* cams;
   const uint32_t* sortedSlots;  // presorted (view, depth, id) order
-  const uint2* rect;
-  const RenderRec* recs;        // read when cull != 0 (the mean)
-  const float4* cullRecs;       // read when cull != 0
-  uint4* itemRecs;              // V * n * 2: per presorted item (rect, mean, cull parameters, slot)
+  const uint4* itemSrc;         // V * n * 2 by slot: (rect, mean, cull parameters, slot) from the projection
+  uint4* itemRecs;              // V * n * 2: the same per presorted item (mean and cull parameters only
+                                // when cull != 0)
   const uint32_t* liveItems;    // presorted items kept (the culled ones left the presort)
   const uint8_t* dropped;
   const uint32_t* viewDrops;
@@ -139,10 +139,6 @@ struct AdamHP {
   float b1, b2, eps, bc1, bc2, minLS, maxLS, maxLogit, reg, shLr;
 };
 
-// floats per (view, splat) chain result: 14 parameter gradients, gated
-// colour gradient (3), view direction (3)
-constexpr int VIEWGRAD_STRIDE = 20;
-
 struct ChainArgs {
   uint32_t n;
   int V;
@@ -150,10 +146,7 @@ struct ChainArgs {
   float* params;
   float* sh;
   int32_t* gradP;
-  const uint2* rect;
-  float* viewGrad;         // V * n * VIEWGRAD_STRIDE: per-(view, splat) chain results
-  uint32_t* visList;       // V * n: per view, indices of the visible splats
-  uint32_t* visCount;      // V counters, cleared before the step
+  const uint2* rect;        // V * n tile rectangles (x = 0xFFFFFFFF: not visible in that view)
   float anisoReg;
   int32_t* gradCam;
   float* gradF;            // optional readout (n * 16)

@@ -121,7 +121,13 @@ __global__ void __launch_bounds__(256, 4) k_project(ProjectArgs a) {  // 4 block
     const uint32_t y1 = u32sat(clampf(floorf((my + rad) / TF), 0.0f, (float)(ty - 1)));
     a.rect[slot] = make_uint2(x0 | (y0 << 16), x1 | (y1 << 16));
     // cull parameters: the tile cull and the rasteriser's warp-block masks
-    a.cullRecs[slot] = cullParams(mx, my, r.r0.z, r.r0.w, r.r1.x, r.r1.y, a.aMin, a.eCut, x0, x1, y0, y1, a.tile);
+    const float4 cq = cullParams(mx, my, r.r0.z, r.r0.w, r.r1.x, r.r1.y, a.aMin, a.eCut, x0, x1, y0, y1, a.tile);
+    a.cullRecs[slot] = cq;
+    // what the expansion needs of this item, in one 32-byte record it
+    // gathers with a single sector read
+    a.itemSrc[2 * slot] = make_uint4(x0 | (y0 << 16), x1 | (y1 << 16), __float_as_uint(mx), __float_as_uint(my));
+    a.itemSrc[2 * slot + 1] = make_uint4(__float_as_uint(cq.x), __float_as_uint(cq.y), __float_as_uint(cq.z),
+                                         (uint32_t)slot);
     // rectangle add on the (tx+1) x (ty+1) difference grid
     int32_t* gd = a.diffGrid + a.gridBase[v];
     const int gw = tx + 1;
@@ -338,17 +344,17 @@ __global__ void __launch_bounds__(256) k_expand(ExpandArgs a) {
   s_run[threadIdx.x] = 0;
   if (valid) {
     // the item's rectangle, mean and cull parameters: gathered by slot in
-    // the count pass and written in presort order, so the key pass reads
-    // them coalesced
+    // the count pass (one 32-byte record the projection wrote) and written
+    // in presort order, so the key pass reads them coalesced
     uint32_t slot;
     uint2 r;
     if (!KEYS) {
       slot = a.sortedSlots[p];
-      r = a.rect[slot];
+      const uint4 s0 = a.itemSrc[2 * slot], s1 = a.itemSrc[2 * slot + 1];
+      r = make_uint2(s0.x, s0.y);
       if (r.x != 0xFFFFFFFFu && a.cull) {
-        const float4 q0 = a.recs[slot].r0;
-        mx = q0.x; my = q0.y;
-        cq = a.cullRecs[slot];
+        mx = __uint_as_float(s0.z); my = __uint_as_float(s0.w);
+        cq = make_float4(__uint_as_float(s1.x), __uint_as_float(s1.y), __uint_as_float(s1.z), 0.0f);
       }
       a.itemRecs[2 * p] = make_uint4(r.x, r.y, __float_as_uint(mx), __float_as_uint(my));
       a.itemRecs[2 * p + 1] = make_uint4(__float_as_uint(cq.x), __float_as_uint(cq.y), __float_as_uint(cq.z), slot);

@@ -420,6 +420,22 @@ __device__ __forceinline__ float2 pairExponent2(const float4& r0, float hC, floa
   return make_float2(fmaxf(e.x, 0.0f), fmaxf(e.y, 0.0f));
 }
 
+// ---- asynchronous staging (cp.async: global -> shared without registers) ----
+// 16-byte copies bypassing L1 (each record is read once per block); a
+// thread's copies complete, in commit order, at its wait_group.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_async_rec(RenderRec* dst, const RenderRec* src) {
+  cp_async16(&dst->r0, &src->r0);
+  cp_async16(&dst->r1, &src->r1);
+  cp_async16(&dst->r2, &src->r2);
+}
+
 #ifndef GS_RASTER_PX2_MIN_BLOCKS
 #define GS_RASTER_PX2_MIN_BLOCKS 8  // resident 128-thread blocks per SM the register allocation must allow
 #endif
@@ -434,13 +450,30 @@ __device__ __forceinline__ float2 pairExponent2(const float4& r0, float hC, floa
 // k_raster<16, BATCH, true, true, false>: the same entries reach every pixel
 // (an 8x8 block skips an entry only when neither of its 8x4 halves can use
 // it), and integer sums do not depend on how pixels are grouped.
+//
+// Staging: each batch of BATCH entries is copied from global to shared
+// memory with cp.async (16-byte copies, no register round trip); the entry
+// ids of the next batch are loaded into registers while the current one is
+// processed, so a batch's staging waits for one gather, not for the id load
+// and then the gather.  Each thread copies its own entries (k = tid,
+// tid + 128) and, in the forward, computes their warp-block masks from its
+// own completed copies before the batch's barrier.  (Double-buffering the
+// records as well -- the next batch copied while the current one is
+// processed -- needs twice the record storage, which at 256 entries drops
+// the block from 8 to 5 resident per SM; measured, it did not pay.)
 template <int BATCH>
 __global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(RasterArgs a) {
   constexpr int NT = 128, NW = 4;
+  constexpr int PER = BATCH >= NT ? BATCH / NT : 1;  // entries a thread stages per batch
   static_assert(BATCH % 32 == 0, "batches hold whole ballot words");
+  static_assert(BATCH <= 2 * NT, "two staged entries per thread");
   __shared__ RenderRec s_rec[BATCH];
+  // the forward's cull parameters and the backward's per-entry sums share storage
+  constexpr int ACC_WORDS = BATCH * 10, CULL_WORDS = BATCH * 4;
+  __shared__ __align__(16) int32_t s_accu[ACC_WORDS > CULL_WORDS ? ACC_WORDS : CULL_WORDS];
+  int32_t* s_acc = s_accu;
+  float4* s_cull = reinterpret_cast<float4*>(s_accu);
   __shared__ uint32_t s_id[BATCH];
-  __shared__ int32_t s_acc[BATCH * 10];
   __shared__ uint32_t s_mask[NW * MASKW];
   __shared__ uint32_t s_live[NW][BATCH / 32];
   __shared__ uint32_t s_item;
@@ -453,8 +486,6 @@ __global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(Ra
   const int ly = (wid >> 1) * 8 + (lane >> 3);  // pixel a; pixel b is 4 rows below
   const float E_CUT = a.eCut, A_MIN = a.aMin;
   uint32_t* wmask = s_mask + wid * MASKW;
-
-  for (int k = tid; k < BATCH * 10; k += NT) s_acc[k] = 0;
 
   for (uint32_t iter = 0;; ++iter) {
     if (tid == 0) s_item = a.workCounter ? atomicAdd(a.workCounter, 1u) : (iter == 0 ? blockIdx.x : 0xFFFFFFFFu);
@@ -486,24 +517,37 @@ __global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(Ra
     bool doneA = !inA, doneB = !inB;
     for (int k = lane; k < MASKW; k += 32) wmask[k] = 0u;
     __syncwarp();
-    // each batch's entry values are loaded while the previous batch is
-    // processed (two per thread), so staging starts with the record gathers
-    static_assert(BATCH <= 2 * NT, "two prefetched values per thread");
-    uint32_t pf0 = s + (uint32_t)tid < e ? a.ids[s + tid] : 0u;
-    uint32_t pf1 = BATCH > NT && s + NT + (uint32_t)tid < e ? a.ids[s + NT + tid] : 0u;
+    // ids of entries [from, to) that this thread stages (k = tid, tid + 128)
+    uint32_t pf[PER];
+    auto load_ids = [&](uint32_t from, uint32_t to) {
+#pragma unroll
+      for (int u = 0; u < PER; ++u) {
+        const uint32_t k = (uint32_t)(u * NT + tid);
+        pf[u] = k < (uint32_t)BATCH && from + k < to ? a.ids[from + k] : 0u;
+      }
+    };
+    load_ids(s, e);
     for (uint32_t base = s; base < e; base += BATCH) {
+      // every warp has finished the previous batch: its buffers may be overwritten
       if (__syncthreads_count(!(doneA && doneB)) == 0) break;
       const uint32_t nb = min((uint32_t)BATCH, e - base);
-      for (uint32_t kb = 0; kb < (uint32_t)BATCH; kb += NT) {
+#pragma unroll
+      for (int u = 0; u < PER; ++u) {
+        const uint32_t k = (uint32_t)(u * NT + tid);
+        if (k < nb) {
+          cp_async_rec(&s_rec[k], recs + pf[u]);
+          cp_async16(&s_cull[k], cullRecs + pf[u]);
+        }
+      }
+      cp_async_commit();
+      load_ids(base + BATCH, e);  // the next batch's ids load while this one is processed
+      cp_async_wait<0>();         // this thread's copies have landed
+#pragma unroll
+      for (int u = 0; u < (BATCH + NT - 1) / NT; ++u) {
+        const uint32_t kb = (uint32_t)(u * NT);
         const uint32_t k = kb + tid;
         uint32_t m = 0;
-        if (k < nb) {
-          const uint32_t id = kb == 0 ? pf0 : pf1;
-          s_id[k] = id;
-          const RenderRec rec = recs[id];
-          s_rec[k] = rec;
-          m = warp_block_mask8(cullRecs[id], rec.r0.x, rec.r0.y, tx, ty);
-        }
+        if (k < nb) m = warp_block_mask8(s_cull[k], s_rec[k].r0.x, s_rec[k].r0.y, tx, ty);
         const uint32_t word = (kb >> 5) + (uint32_t)wid;
 #pragma unroll
         for (int w = 0; w < NW; ++w) {
@@ -512,11 +556,6 @@ __global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(Ra
         }
       }
       __syncthreads();
-      {
-        const uint32_t nx = base + BATCH;
-        pf0 = nx + (uint32_t)tid < e ? a.ids[nx + tid] : 0u;
-        pf1 = BATCH > NT && nx + NT + (uint32_t)tid < e ? a.ids[nx + NT + tid] : 0u;
-      }
       if (!__all_sync(FULL, doneA && doneB)) {
         const uint32_t rbase = base - s;
         for (uint32_t jw = 0; jw < nb; jw += 32) {
@@ -555,7 +594,6 @@ __global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(Ra
           if (__all_sync(FULL, doneA && doneB)) break;
         }
       }
-      __syncthreads();
     }
     C0 = __fadd2_rn(C0, __fmul2_rn(T, bc2(c.bg[0])));
     C1 = __fadd2_rn(C1, __fmul2_rn(T, bc2(c.bg[1])));
@@ -637,112 +675,128 @@ __global__ void __launch_bounds__(128, GS_RASTER_PX2_MIN_BLOCKS) k_raster_px2(Ra
     uint32_t endMax = 0;
 #pragma unroll
     for (int w = 0; w < NW; ++w) endMax = max(endMax, s_endmax[w]);
+    // the forward's cull parameters shared storage with the per-entry sums:
+    // every reader of them has passed the barrier above
+    for (int k = tid; k < BATCH * 10; k += NT) s_acc[k] = 0;
 
     // ---- backward (shaders.js:632-700) ----
     float2 S0 = __fmul2_rn(bc2(c.bg[0]), T), S1 = __fmul2_rn(bc2(c.bg[1]), T), S2 = __fmul2_rn(bc2(c.bg[2]), T);
     float2 Ta = T;
     int32_t* gradP = a.gradP + (size_t)v * a.n * GP_STRIDE;
+    // batches run back to front: [lo, hi) with hi = endMax, then hi = lo;
+    // each batch's ids are loaded while the batch before it is processed
+    auto lo_of = [](uint32_t hi) { return hi > (uint32_t)BATCH ? hi - (uint32_t)BATCH : 0u; };
+    if (endMax > 0) load_ids(s + lo_of(endMax), s + endMax);
     for (uint32_t hi = endMax; hi > 0;) {
-      const uint32_t lo = hi > (uint32_t)BATCH ? hi - BATCH : 0u;
+      const uint32_t lo = lo_of(hi);
       const uint32_t nb = hi - lo;
-      __syncthreads();
-      for (uint32_t k = tid; k < nb; k += NT) {
-        const uint32_t id = a.ids[s + lo + k];
-        s_id[k] = id;
-        s_rec[k] = recs[id];
-      }
-      __syncthreads();
-      for (int32_t w = (int32_t)((hi - 1) >> 5); w >= (int32_t)(lo >> 5); --w) {
-        const uint32_t wb = (uint32_t)w << 5;
-        uint32_t word = (uint32_t)w < (uint32_t)MASKW ? wmask[w] : FULL;
-        if (wb + 32u > hi) word &= FULL >> (wb + 32u - hi);
-        if (wb < lo) word &= FULL << (lo - wb);
-        while (word) {
-          const uint32_t bit = 31u - (uint32_t)__clz(word);
-          word &= ~(1u << bit);
-          const uint32_t j = wb + bit;
-          const RenderRec& rr = s_rec[j - lo];
-          const float4 r0 = rr.r0;
-          const float4 r1 = rr.r1;
-          const float4 r2 = rr.r2;
-          const float dx = px - r0.x;
-          const float2 dy = __fadd2_rn(py, bc2(-r0.y));
-          float2 Bdy;
-          const float2 ee = pairExponent2(r0, r1.x, dx, dy, Bdy);
-          const float2 G = gexp2(make_float2(-fminf(ee.x, 80.0f), -fminf(ee.y, 80.0f)));
-          const float2 araw = __fmul2_rn(bc2(r1.y), G);
-          const float2 alpha = make_float2(fminf(0.99f, araw.x), fminf(0.99f, araw.y));
-          const bool c2a = j < myEndA && ee.x <= E_CUT && alpha.x >= A_MIN;
-          const bool c2b = j < myEndB && ee.y <= E_CUT && alpha.y >= A_MIN;
-          const uint32_t balA = __ballot_sync(FULL, c2a), balB = __ballot_sync(FULL, c2b);
-          if ((balA | balB) == 0u) continue;
-          const float2 inv = rcp_unit2(__fadd2_rn(bc2(1.0f), make_float2(-alpha.x, -alpha.y)));
-          const float2 Tb = __fmul2_rn(Ta, inv);
-          const float2 at = __fmul2_rn(alpha, Tb);
-          const float2 aT = make_float2(c2a ? at.x : 0.0f, c2b ? at.y : 0.0f);
-          const float2 g0 = __ffma2_rn(bc2(r1.z), Tb, __fmul2_rn(make_float2(-S0.x, -S0.y), inv));
-          const float2 g1 = __ffma2_rn(bc2(r1.w), Tb, __fmul2_rn(make_float2(-S1.x, -S1.y), inv));
-          const float2 g2 = __ffma2_rn(bc2(r2.x), Tb, __fmul2_rn(make_float2(-S2.x, -S2.y), inv));
-          // galpha * 2^14, accumulated from gC * 2^14
-          const float2 gal16r = __ffma2_rn(g16_2, g2, __ffma2_rn(g16_1, g1, __fmul2_rn(g16_0, g0)));
-          const float2 gal16 = make_float2(c2a && !(araw.x > 0.99f) ? gal16r.x : 0.0f,
-                                           c2b && !(araw.y > 0.99f) ? gal16r.y : 0.0f);
-          const float2 ga16 = __fmul2_rn(gal16, araw);
-          const float cA = r0.z + r0.z, cC = r1.x + r1.x;
-          const float2 gq16 = __fmul2_rn(ga16, bc2(r2.z));
-          const float2 gqx16 = __fmul2_rn(gq16, bc2(dx));
-          float2 xs[10];
-          xs[0] = __fmul2_rn(ga16, __ffma2_rn(bc2(cA), bc2(dx), Bdy));
-          xs[1] = __fmul2_rn(ga16, __ffma2_rn(bc2(r0.w), bc2(dx), __fmul2_rn(bc2(cC), dy)));
-          xs[2] = __fmul2_rn(gqx16, bc2(dx));
-          xs[3] = __fmul2_rn(__fmul2_rn(gqx16, dy), bc2(2.0f));
-          xs[4] = __fmul2_rn(__fmul2_rn(gq16, dy), dy);
-          xs[5] = __fmul2_rn(__fmul2_rn(gal16, bc2(r2.y)), G);
-          xs[6] = __fmul2_rn(ga16, bc2(r2.w));
-          xs[7] = __fmul2_rn(g16_0, aT);
-          xs[8] = __fmul2_rn(g16_1, aT);
-          xs[9] = __fmul2_rn(g16_2, aT);
-          uint32_t rsum[10];
-          if (!__all_sync(FULL, fabsf(gal16.x) < 1.0e7f && fabsf(gal16.y) < 1.0e7f && pixFast)) {
+      __syncthreads();  // the previous batch's processing and flush are over
 #pragma unroll
-            for (int k = 0; k < 10; ++k)
-              xs[k] = make_float2(fminf(fmaxf(xs[k].x, -1.0e9f), 1.0e9f), fminf(fmaxf(xs[k].y, -1.0e9f), 1.0e9f));
-          }
-          // a half of the block with no compositing pixel has every value 0
-          if (balA != 0u && balB != 0u) {
-#pragma unroll
-            for (int k = 0; k < 10; ++k)
-              rsum[k] = __reduce_add_sync(FULL, (uint32_t)__float2int_rz(xs[k].x) + (uint32_t)__float2int_rz(xs[k].y));
-          } else if (balA != 0u) {
-#pragma unroll
-            for (int k = 0; k < 10; ++k) rsum[k] = __reduce_add_sync(FULL, (uint32_t)__float2int_rz(xs[k].x));
-          } else {
-#pragma unroll
-            for (int k = 0; k < 10; ++k) rsum[k] = __reduce_add_sync(FULL, (uint32_t)__float2int_rz(xs[k].y));
-          }
-          // a pixel that does not composite has aT = 0: S stays exactly as it is
-          S0 = __ffma2_rn(bc2(r1.z), aT, S0);
-          S1 = __ffma2_rn(bc2(r1.w), aT, S1);
-          S2 = __ffma2_rn(bc2(r2.x), aT, S2);
-          Ta = make_float2(c2a ? Tb.x : Ta.x, c2b ? Tb.y : Ta.y);
-          if (lane == 0) {
-            int4* st = reinterpret_cast<int4*>(s_stage[wid]);
-            st[0] = make_int4((int)rsum[0], (int)rsum[1], (int)rsum[2], (int)rsum[3]);
-            st[1] = make_int4((int)rsum[4], (int)rsum[5], (int)rsum[6], (int)rsum[7]);
-            reinterpret_cast<int2*>(s_stage[wid])[4] = make_int2((int)rsum[8], (int)rsum[9]);
-          }
-          __syncwarp();
-          if (lane < 10) atomicAdd(&s_acc[(j - lo) * 10 + (uint32_t)lane], s_stage[wid][lane]);
-          __syncwarp();
+      for (int u = 0; u < PER; ++u) {
+        const uint32_t k = (uint32_t)(u * NT + tid);
+        if (k < nb) {
+          s_id[k] = pf[u];
+          cp_async_rec(&s_rec[k], recs + pf[u]);
         }
       }
+      cp_async_commit();
+      if (lo > 0) load_ids(s + lo_of(lo), s + lo);
+      cp_async_wait<0>();
       __syncthreads();
-      for (uint32_t k = tid; k < nb * 10; k += NT) {
-        const int32_t val = s_acc[k];
-        if (val) {
-          const uint32_t jl = k / 10, slot = k - jl * 10;
-          atomicAdd(&gradP[(size_t)s_id[jl] * GP_STRIDE + slot], val);
-          s_acc[k] = 0;
+      {
+        const RenderRec* srec = s_rec;
+        for (int32_t w = (int32_t)((hi - 1) >> 5); w >= (int32_t)(lo >> 5); --w) {
+          const uint32_t wb = (uint32_t)w << 5;
+          uint32_t word = (uint32_t)w < (uint32_t)MASKW ? wmask[w] : FULL;
+          if (wb + 32u > hi) word &= FULL >> (wb + 32u - hi);
+          if (wb < lo) word &= FULL << (lo - wb);
+          while (word) {
+            const uint32_t bit = 31u - (uint32_t)__clz(word);
+            word &= ~(1u << bit);
+            const uint32_t j = wb + bit;
+            const RenderRec& rr = srec[j - lo];
+            const float4 r0 = rr.r0;
+            const float4 r1 = rr.r1;
+            const float4 r2 = rr.r2;
+            const float dx = px - r0.x;
+            const float2 dy = __fadd2_rn(py, bc2(-r0.y));
+            float2 Bdy;
+            const float2 ee = pairExponent2(r0, r1.x, dx, dy, Bdy);
+            const float2 G = gexp2(make_float2(-fminf(ee.x, 80.0f), -fminf(ee.y, 80.0f)));
+            const float2 araw = __fmul2_rn(bc2(r1.y), G);
+            const float2 alpha = make_float2(fminf(0.99f, araw.x), fminf(0.99f, araw.y));
+            const bool c2a = j < myEndA && ee.x <= E_CUT && alpha.x >= A_MIN;
+            const bool c2b = j < myEndB && ee.y <= E_CUT && alpha.y >= A_MIN;
+            const uint32_t balA = __ballot_sync(FULL, c2a), balB = __ballot_sync(FULL, c2b);
+            if ((balA | balB) == 0u) continue;
+            const float2 inv = rcp_unit2(__fadd2_rn(bc2(1.0f), make_float2(-alpha.x, -alpha.y)));
+            const float2 Tb = __fmul2_rn(Ta, inv);
+            const float2 at = __fmul2_rn(alpha, Tb);
+            const float2 aT = make_float2(c2a ? at.x : 0.0f, c2b ? at.y : 0.0f);
+            const float2 g0 = __ffma2_rn(bc2(r1.z), Tb, __fmul2_rn(make_float2(-S0.x, -S0.y), inv));
+            const float2 g1 = __ffma2_rn(bc2(r1.w), Tb, __fmul2_rn(make_float2(-S1.x, -S1.y), inv));
+            const float2 g2 = __ffma2_rn(bc2(r2.x), Tb, __fmul2_rn(make_float2(-S2.x, -S2.y), inv));
+            // galpha * 2^14, accumulated from gC * 2^14
+            const float2 gal16r = __ffma2_rn(g16_2, g2, __ffma2_rn(g16_1, g1, __fmul2_rn(g16_0, g0)));
+            const float2 gal16 = make_float2(c2a && !(araw.x > 0.99f) ? gal16r.x : 0.0f,
+                                             c2b && !(araw.y > 0.99f) ? gal16r.y : 0.0f);
+            const float2 ga16 = __fmul2_rn(gal16, araw);
+            const float cA = r0.z + r0.z, cC = r1.x + r1.x;
+            const float2 gq16 = __fmul2_rn(ga16, bc2(r2.z));
+            const float2 gqx16 = __fmul2_rn(gq16, bc2(dx));
+            float2 xs[10];
+            xs[0] = __fmul2_rn(ga16, __ffma2_rn(bc2(cA), bc2(dx), Bdy));
+            xs[1] = __fmul2_rn(ga16, __ffma2_rn(bc2(r0.w), bc2(dx), __fmul2_rn(bc2(cC), dy)));
+            xs[2] = __fmul2_rn(gqx16, bc2(dx));
+            xs[3] = __fmul2_rn(__fmul2_rn(gqx16, dy), bc2(2.0f));
+            xs[4] = __fmul2_rn(__fmul2_rn(gq16, dy), dy);
+            xs[5] = __fmul2_rn(__fmul2_rn(gal16, bc2(r2.y)), G);
+            xs[6] = __fmul2_rn(ga16, bc2(r2.w));
+            xs[7] = __fmul2_rn(g16_0, aT);
+            xs[8] = __fmul2_rn(g16_1, aT);
+            xs[9] = __fmul2_rn(g16_2, aT);
+            uint32_t rsum[10];
+            if (!__all_sync(FULL, fabsf(gal16.x) < 1.0e7f && fabsf(gal16.y) < 1.0e7f && pixFast)) {
+#pragma unroll
+              for (int k = 0; k < 10; ++k)
+                xs[k] = make_float2(fminf(fmaxf(xs[k].x, -1.0e9f), 1.0e9f), fminf(fmaxf(xs[k].y, -1.0e9f), 1.0e9f));
+            }
+            // a half of the block with no compositing pixel has every value 0
+            if (balA != 0u && balB != 0u) {
+#pragma unroll
+              for (int k = 0; k < 10; ++k)
+                rsum[k] = __reduce_add_sync(FULL, (uint32_t)__float2int_rz(xs[k].x) + (uint32_t)__float2int_rz(xs[k].y));
+            } else if (balA != 0u) {
+#pragma unroll
+              for (int k = 0; k < 10; ++k) rsum[k] = __reduce_add_sync(FULL, (uint32_t)__float2int_rz(xs[k].x));
+            } else {
+#pragma unroll
+              for (int k = 0; k < 10; ++k) rsum[k] = __reduce_add_sync(FULL, (uint32_t)__float2int_rz(xs[k].y));
+            }
+            // a pixel that does not composite has aT = 0: S stays exactly as it is
+            S0 = __ffma2_rn(bc2(r1.z), aT, S0);
+            S1 = __ffma2_rn(bc2(r1.w), aT, S1);
+            S2 = __ffma2_rn(bc2(r2.x), aT, S2);
+            Ta = make_float2(c2a ? Tb.x : Ta.x, c2b ? Tb.y : Ta.y);
+            if (lane == 0) {
+              int4* st = reinterpret_cast<int4*>(s_stage[wid]);
+              st[0] = make_int4((int)rsum[0], (int)rsum[1], (int)rsum[2], (int)rsum[3]);
+              st[1] = make_int4((int)rsum[4], (int)rsum[5], (int)rsum[6], (int)rsum[7]);
+              reinterpret_cast<int2*>(s_stage[wid])[4] = make_int2((int)rsum[8], (int)rsum[9]);
+            }
+            __syncwarp();
+            if (lane < 10) atomicAdd(&s_acc[(j - lo) * 10 + (uint32_t)lane], s_stage[wid][lane]);
+            __syncwarp();
+          }
+        }
+        __syncthreads();
+        for (uint32_t k = tid; k < nb * 10; k += NT) {
+          const int32_t val = s_acc[k];
+          if (val) {
+            const uint32_t jl = k / 10, slot = k - jl * 10;
+            atomicAdd(&gradP[(size_t)s_id[jl] * GP_STRIDE + slot], val);
+            s_acc[k] = 0;
+          }
         }
       }
       hi = lo;
