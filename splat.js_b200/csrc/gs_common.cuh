@@ -60,6 +60,17 @@ struct __align__(16) RenderRec {
   float4 r0, r1, r2;
 };
 
+// ---- asynchronous staging (cp.async: global -> shared without registers) ----
+// 16-byte copies bypassing L1 (each record is read once per block); a
+// thread's copies complete, in commit order, at its wait_group.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // ---- canonical scalar functions --------------------------------------------
 // exp(x), |x| <= 87: Cody-Waite reduction x = k ln2 + r with ln2 split in a
 // 16-bit head and a tail, e^r by its degree-7 Taylor series on

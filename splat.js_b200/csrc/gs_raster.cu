@@ -420,16 +420,6 @@ __device__ __forceinline__ float2 pairExponent2(const float4& r0, float hC, floa
   return make_float2(fmaxf(e.x, 0.0f), fmaxf(e.y, 0.0f));
 }
 
-// ---- asynchronous staging (cp.async: global -> shared without registers) ----
-// 16-byte copies bypassing L1 (each record is read once per block); a
-// thread's copies complete, in commit order, at its wait_group.
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 __device__ __forceinline__ void cp_async_rec(RenderRec* dst, const RenderRec* src) {
   cp_async16(&dst->r0, &src->r0);
   cp_async16(&dst->r1, &src->r1);

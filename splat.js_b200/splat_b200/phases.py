@@ -13,6 +13,10 @@ rest).  Work units per splat and view: projection 64 + 12K read, 64 + 4
 written; chain 232 + 24K; Adam 28 bytes per learnable scalar (14 + 3K per
 splat); sort 172 bytes per reference (tile, splat) entry; raster 96 flop
 per pair.
+
+--profile-window sets the workload up, warms up three steps, then runs ONE
+batched step between cudaProfilerStart/Stop (for ncu --profile-from-start
+off) and prints no phase line.
 """
 from __future__ import annotations
 
@@ -42,7 +46,8 @@ def parse(argv=None):
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--batch-depth", type=int, default=256, choices=[64, 128, 256])
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--hbm-gbs", type=float, default=6542.7, help="measured HBM copy bandwidth, GB/s")
+    ap.add_argument("--hbm-gbs", type=float, default=6534.5, help="measured HBM copy bandwidth, GB/s")
+    ap.add_argument("--profile-window", action="store_true")
     return ap.parse_args(argv)
 
 
@@ -73,6 +78,15 @@ def main(argv=None):
     for k in range(3):
         t.stepBatch(batch(k))
     N.check(L.gs_sync(h), h)
+    if a.profile_window:
+        import torch
+        torch.cuda.profiler.start()
+        t.stepBatch(batch(3))
+        N.check(L.gs_sync(h), h)
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profile_window": "one batched step", "views": batch(3), "splats": n,
+                          "sh_degree": a.sh_degree}))
+        return
     t0 = time.perf_counter()
     for k in range(a.steps):
         t.stepBatch(batch(3 + k))
