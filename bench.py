@@ -40,8 +40,10 @@ from splat_b200.clocks import ClockSampler  # noqa: E402
 METRIC = "train views/s @1M splats 1080p, batched vs plain step, 1 B200, grads within 1e-4"
 FLOP_PER_PAIR = 26 + 70   # raster forward + backward per evaluated pixel-entry pair (FFMA = 2)
 # DRAM bytes (read + write) of one raster launch over an 8-view batch at the
-# default workload, from one ncu capture (not measured live)
-RASTER_DRAM_BYTES_8VIEW = 2.013450e9 + 0.524951e9
+# default workload: one ncu capture of a 2-view launch of the same scene
+# (two 1080p ring views; 311.98 MB read + 95.85 MB written), scaled by the
+# view count (not measured live)
+RASTER_DRAM_BYTES_8VIEW = (311.978240e6 + 95.846656e6) * 4
 
 
 def parse():
@@ -444,8 +446,8 @@ def run_ours(args):
                              "frac": achieved / peak.value if peak.value else None,
                              "traffic": RASTER_DRAM_BYTES_8VIEW if (B == 8 and n == 1_000_000 and args.width == 1920)
                              else None,
-                             "traffic_source": "one ncu capture of the raster over an 8-view step (cameras 0-7) "
-                                               "of this workload",
+                             "traffic_source": "one ncu capture of the raster over a 2-view step of this scene "
+                                               "(two 1080p ring views), scaled to 8 views",
                              "peak_source": "gs_probe_fp32_peak FFMA kernel on this GPU (measured)",
                              "work": f"{FLOP_PER_PAIR} flop per pixel-entry pair P of the reference's tile lists "
                                      "(pairs up to each pixel's termination index); the step walks culled lists "
