@@ -2,16 +2,15 @@
 // screen-space gradients to parameter gradients (shaders.js:704-949), fused
 // with Adam (shaders.js:984-1036) and SH-Adam (shaders.js:952-982).
 //
-// One kernel, one thread per splat.  The thread reads the splat's
-// parameters and SH coefficients once, then for every view of the batch in
-// view order decodes the splat's fixed-point screen-space gradients (clearing
-// them for the next step), chains them through that view's camera and adds
-// the result to its running sums; the block then runs Adam and SH-Adam over
-// its splats with coalesced parameter and moment traffic.  The reference runs
-// chain, Adam and SH-Adam as three dispatches with gradF / shGrad
-// round-tripping through memory; here the summed gradients stay on chip
-// unless the caller asks for them (gradient readout for checks).  Operation
-// order follows the WGSL.
+// Two passes.  Pass 1 (one thread per (view, splat)) decodes each visible
+// splat's fixed-point screen-space gradients (clearing them for the next
+// step) and chains them through that view's camera.  Pass 2 (one thread per
+// splat) sums the views' parameter gradients in view order and runs Adam
+// and SH-Adam once, with coalesced parameter and moment traffic.  The
+// reference runs chain, Adam and SH-Adam as three dispatches with gradF /
+// shGrad round-tripping through memory; here the summed gradients stay on
+// chip unless the caller asks for them (gradient readout for checks).
+// Operation order follows the WGSL.
 #include "gs_geom.cuh"
 #include "gs_kernels.h"
 
@@ -232,79 +231,80 @@ __device__ __forceinline__ void adamParam(const AdamHP& h, int slot, float& p, f
 }
 
 #ifndef GS_CHAIN_MIN_BLOCKS
-#define GS_CHAIN_MIN_BLOCKS 4  // resident 128-thread blocks per SM the register allocation must allow
+#define GS_CHAIN_MIN_BLOCKS 4  // resident 128-thread blocks per SM the register allocation must allow (no spills)
 #endif
 
-// One thread per splat: the chain for every view of the batch in view order,
-// then Adam and SH-Adam.  The splat's parameters and SH coefficients are read
-// once for all views; per view only its visibility (the tile rectangle) and
-// its fixed-point screen-space gradients (cleared for the next step) are
-// read.  The per-view parameter gradients are summed in view order from zero
-// into the thread's own shared-memory row (views where the splat is not
-// visible would add +0 and are skipped); the gated colour gradient times the
-// SH basis is summed the same way.  Camera gradients are summed per warp and
-// view in fixed point (order-independent) with one atomic each.  The block
-// then updates its 128 splats through shared memory, one float per thread
-// per step, so every parameter and moment access is coalesced.
+// Visible-item lists: for each view, the indices of the splats whose
+// rectangle survived projection, compacted with one atomic per block.  The
+// order inside a list follows the blocks' atomics (roughly ascending), which
+// pass 1 uses only for memory locality: each item's results go to its own
+// slot and camera gradients are integer sums, so no result depends on it.
+__global__ void __launch_bounds__(256) k_visible_list(ChainArgs a, uint32_t blocksPerView) {
+  __shared__ uint32_t s_warp[8];
+  __shared__ uint32_t s_base;
+  const uint32_t v = blockIdx.x / blocksPerView;
+  const uint32_t i = (blockIdx.x - v * blocksPerView) * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const bool vis = i < a.n && a.rect[(size_t)v * a.n + i].x != 0xFFFFFFFFu;
+  const uint32_t b = __ballot_sync(0xFFFFFFFFu, vis);
+  if (lane == 0) s_warp[wid] = (uint32_t)__popc(b);
+  __syncthreads();
+  if (threadIdx.x == 0) {  // one atomic per block
+    uint32_t t = 0;
+    for (int w = 0; w < 8; ++w) { const uint32_t c = s_warp[w]; s_warp[w] = t; t += c; }
+    s_base = t ? atomicAdd(&a.visCount[v], t) : 0u;
+  }
+  __syncthreads();
+  if (vis) a.visList[(size_t)v * a.n + s_base + s_warp[wid] + (uint32_t)__popc(b & ((1u << lane) - 1u))] = i;
+}
+
+// Pass 1: one thread per visible (view, splat) item of the lists above.
+// Blocks are ordered list block major, view minor, so the views' items of
+// similar splat indices run together and their parameters and SH
+// coefficients are mostly read from DRAM once.  A visible splat's screen-space
+// gradients are decoded (and cleared for the next step) and chained through
+// the view's camera; the result -- the 14 parameter gradients, the gated
+// colour gradient dRGB and the view direction (from which the SH basis Y is
+// recomputed) -- goes to viewGrad[slot] for pass 2.  Camera gradients are
+// summed per warp in fixed point (order-independent) with one atomic each.
 template <int DEG>
-__global__ void __launch_bounds__(128, GS_CHAIN_MIN_BLOCKS) k_chain_step(ChainArgs a) {
+__global__ void __launch_bounds__(128, GS_CHAIN_MIN_BLOCKS) k_chain_view(ChainArgs a) {
   constexpr int K = DEG > 0 ? (DEG + 1) * (DEG + 1) - 1 : 0;
-  constexpr int SHN = 3 * K;
-  constexpr int GROW = 17;                             // odd row strides: conflict-free row access
-  constexpr int SROW = SHN > 0 ? (SHN | 1) : 1;
-  constexpr uint32_t SHD = SHN > 0 ? SHN : 1;          // divisor (the SH loops are empty when SHN = 0)
-  __shared__ float s_g[128 * GROW];
-  __shared__ float s_sh[SHN > 0 ? 128 * SROW : 1];
-  __shared__ DevCam s_cams[MAX_VIEWS];
-  const uint32_t i0 = blockIdx.x * blockDim.x;
-  const uint32_t i = i0 + threadIdx.x;
-  const int t = threadIdx.x, lane = t & 31;
-  const bool have = i < a.n;
-  copy_cams(s_cams, a.cams, a.V);
-  // visibility in every view (16 independent loads in flight)
-  uint32_t visMask = 0;
-#pragma unroll
-  for (int v = 0; v < MAX_VIEWS; ++v)
-    if (v < a.V && have && a.rect[(size_t)v * a.n + i].x != 0xFFFFFFFFu) visMask |= 1u << v;
+  const uint32_t sb = blockIdx.x / (uint32_t)a.V;
+  const int v = (int)(blockIdx.x - sb * (uint32_t)a.V);
+  const uint32_t pos = sb * blockDim.x + threadIdx.x;
+  const uint32_t cnt = a.visCount[v];
+  if (sb * blockDim.x >= cnt) return;  // the whole block is past the list (uniform)
+  const bool have = pos < cnt;
+  const uint32_t i = have ? a.visList[(size_t)v * a.n + pos] : 0u;
+  const int lane = threadIdx.x & 31;
+  // the block's camera in shared memory (read once, not re-fetched from
+  // global memory around every store); every thread issues its own loads
+  // before the barrier that publishes it
+  __shared__ DevCam s_cam;
+  copy_cams(&s_cam, a.cams + v, 1);
+  const size_t slot = (size_t)v * a.n + i;
+  int4 q0 = make_int4(0, 0, 0, 0), q1 = q0, q2 = q0;
   float P[16];
-#pragma unroll
-  for (int k = 0; k < 16; ++k) P[k] = 0.0f;
   if (have) {
+    const int4* G4 = reinterpret_cast<const int4*>(a.gradP + slot * GP_STRIDE);
+    q0 = G4[0]; q1 = G4[1]; q2 = G4[2];
     const float4* P4 = reinterpret_cast<const float4*>(a.params + (size_t)i * STRIDE);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const float4 q = P4[k];
-      P[4 * k] = q.x; P[4 * k + 1] = q.y; P[4 * k + 2] = q.z; P[4 * k + 3] = q.w;
+      const float4 t = __ldg(P4 + k);
+      P[4 * k] = t.x; P[4 * k + 1] = t.y; P[4 * k + 2] = t.z; P[4 * k + 3] = t.w;
     }
   }
-  float* gRow = s_g + t * GROW;
-  float* shRow = s_sh + t * SROW;
-#pragma unroll
-  for (int k = 0; k < 16; ++k) gRow[k] = 0.0f;
-#pragma unroll
-  for (int k = 0; k < SHN; ++k) shRow[k] = 0.0f;
-  // the first visible view's screen-space gradients; each view then fetches the next one's
-  int4 nq0 = make_int4(0, 0, 0, 0), nq1 = nq0, nq2 = nq0;
-  if (visMask) {
-    const int4* G4 = reinterpret_cast<const int4*>(a.gradP + ((size_t)(__ffs(visMask) - 1) * a.n + i) * GP_STRIDE);
-    nq0 = G4[0]; nq1 = G4[1]; nq2 = G4[2];
-  }
   __syncthreads();
-  const float* shp = K > 0 && have ? a.sh + (size_t)i * 3 * K : nullptr;
-  for (int v = 0; v < a.V; ++v) {
-    const DevCam& c = s_cams[v];
-    CamGrad7 cg = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f};
-    if ((visMask >> v) & 1u) {
-      const int4 q0 = nq0, q1 = nq1, q2 = nq2;
-      int4* G4 = reinterpret_cast<int4*>(a.gradP + ((size_t)v * a.n + i) * GP_STRIDE);
+  const DevCam& c = s_cam;
+  CamGrad7 cg = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f};
+  if (have) {
+    {
+      int4* G4 = reinterpret_cast<int4*>(a.gradP + slot * GP_STRIDE);
       G4[0] = make_int4(0, 0, 0, 0);
       G4[1] = make_int4(0, 0, 0, 0);
       G4[2] = make_int4(0, 0, 0, 0);
-      const uint32_t rest = visMask & ~((2u << v) - 1u);
-      if (rest) {
-        const int4* N4 = reinterpret_cast<const int4*>(a.gradP + ((size_t)(__ffs(rest) - 1) * a.n + i) * GP_STRIDE);
-        nq0 = N4[0]; nq1 = N4[1]; nq2 = N4[2];
-      }
       const int32_t qi[10] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y};
       float gp[10];
 #pragma unroll
@@ -322,30 +322,86 @@ __global__ void __launch_bounds__(128, GS_CHAIN_MIN_BLOCKS) k_chain_step(ChainAr
         const float lmax = cmid + sqrtf(fmaxf(cmid * cmid - (cva * cvc - g.vb * g.vb), 0.0f));
         const float cden = 1.0f + lmax;
         gp[2] = gp[2] * cden; gp[3] = gp[3] * cden; gp[4] = gp[4] * cden;
+        const float* shp = K > 0 ? a.sh + (size_t)i * 3 * K : nullptr;
         chainOne<DEG>(c, P, g, gp, shp, a.anisoReg, gF, dRGB, Y, vd, aK, cg);
       }
+      float4* o = reinterpret_cast<float4*>(a.viewGrad + slot * VIEWGRAD_STRIDE);
+      o[0] = make_float4(gF[0], gF[1], gF[2], gF[3]);
+      o[1] = make_float4(gF[4], gF[5], gF[6], gF[7]);
+      o[2] = make_float4(gF[8], gF[9], gF[10], gF[11]);
+      o[3] = make_float4(gF[12], gF[13], dRGB[0], dRGB[1]);
+      o[4] = make_float4(dRGB[2], vd[0], vd[1], vd[2]);
+    }
+  }
+  // camera gradients: warp sums of the fixed-point values, one atomic each
+  if (c.train) {
+    const float cv[7] = {cg.w[0], cg.w[1], cg.w[2], cg.t[0], cg.t[1], cg.t[2], cg.logf};
 #pragma unroll
-      for (int k = 0; k < 14; ++k) gRow[k] = gRow[k] + gF[k];
-      if (K > 0) {
-#pragma unroll
-        for (int ch = 0; ch < 3; ++ch)
-#pragma unroll
-          for (int k = 0; k < K; ++k)
-            shRow[ch * K + k] = shRow[ch * K + k] + (k < aK ? dRGB[ch] * Y[k] : 0.0f);
+    for (int k = 0; k < 7; ++k) {
+      const uint32_t r = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)fixq(cv[k], FIXCAM));
+      if (lane == 0 && r) {
+        const uint32_t idx = k < 6 ? c.camIdx * 8u + (uint32_t)k : c.ncams * 8u;
+        atomicAdd(&a.gradCam[idx], (int32_t)r);
       }
     }
-    // camera gradients: warp sums of the fixed-point values, one atomic each
-    if (c.train) {
-      const float cv[7] = {cg.w[0], cg.w[1], cg.w[2], cg.t[0], cg.t[1], cg.t[2], cg.logf};
+  }
+}
+
+// Pass 2: one thread per splat sums its views' gradients in view order from
+// zero (views where the splat was not visible add +0, which changes no sum,
+// and are skipped), then the block updates its 128 splats with Adam and
+// SH-Adam through shared memory, one float per thread per step, so every
+// global access is coalesced.
+template <int DEG>
+__global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
+  constexpr int K = DEG > 0 ? (DEG + 1) * (DEG + 1) - 1 : 0;
+  constexpr int SHN = 3 * K;
+  constexpr int GROW = 17;                 // padded rows: conflict-free column writes
+  constexpr int SROW = SHN > 0 ? SHN + 1 : 1;
+  constexpr uint32_t SHD = SHN > 0 ? SHN : 1;  // divisor (the SH loops are empty when SHN = 0)
+  __shared__ float s_g[128 * GROW];
+  __shared__ float s_sh[SHN > 0 ? 128 * SROW : 1];
+  const uint32_t i0 = blockIdx.x * blockDim.x;
+  const uint32_t i = i0 + threadIdx.x;
+  const int t = threadIdx.x;
+  {
+    float gFa[14];
+    float shA[SHN > 0 ? SHN : 1];
 #pragma unroll
-      for (int k = 0; k < 7; ++k) {
-        const uint32_t r = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)fixq(cv[k], FIXCAM));
-        if (lane == 0 && r) {
-          const uint32_t idx = k < 6 ? c.camIdx * 8u + (uint32_t)k : c.ncams * 8u;
-          atomicAdd(&a.gradCam[idx], (int32_t)r);
+    for (int k = 0; k < 14; ++k) gFa[k] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < SHN; ++k) shA[k] = 0.0f;
+    if (i < a.n) {
+      for (int v = 0; v < a.V; ++v) {
+        const size_t slot = (size_t)v * a.n + i;
+        if (a.rect[slot].x == 0xFFFFFFFFu) continue;
+        const float4* q = reinterpret_cast<const float4*>(a.viewGrad + slot * VIEWGRAD_STRIDE);
+        const float4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
+        const float gF[14] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w,
+                              q2.x, q2.y, q2.z, q2.w, q3.x, q3.y};
+#pragma unroll
+        for (int k = 0; k < 14; ++k) gFa[k] = gFa[k] + gF[k];
+        if (K > 0) {
+          const float4 q4 = q[4];
+          const float dRGB[3] = {q3.z, q3.w, q4.x};
+          const float vd[3] = {q4.y, q4.z, q4.w};
+          float Y[15];
+          shBasis<DEG>(vd, Y);
+          const int aK = shActiveK(a.cams[v], K);
+#pragma unroll
+          for (int ch = 0; ch < 3; ++ch)
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+              shA[ch * K + k] = shA[ch * K + k] + (k < aK ? dRGB[ch] * Y[k] : 0.0f);
         }
       }
     }
+#pragma unroll
+    for (int k = 0; k < 14; ++k) s_g[t * GROW + k] = gFa[k];
+    s_g[t * GROW + 14] = 0.0f;
+    s_g[t * GROW + 15] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < SHN; ++k) s_sh[t * SROW + k] = shA[k];
   }
   __syncthreads();
   const uint32_t cnt = a.n - i0 < 128u ? a.n - i0 : 128u;  // splats of this block
@@ -413,11 +469,14 @@ __global__ void __launch_bounds__(128, GS_CHAIN_MIN_BLOCKS) k_chain_step(ChainAr
 void launch_chain_adam(const ChainArgs& a, int deg, cudaStream_t s) {
   const unsigned blocks = (a.n + 127) / 128;
   if (blocks == 0) return;
+  const unsigned g1 = blocks * (unsigned)a.V;
+  const unsigned bpv = (a.n + 255) / 256;
+  k_visible_list<<<bpv * (unsigned)a.V, 256, 0, s>>>(a, bpv);
   switch (deg) {
-    case 0: k_chain_step<0><<<blocks, 128, 0, s>>>(a); break;
-    case 1: k_chain_step<1><<<blocks, 128, 0, s>>>(a); break;
-    case 2: k_chain_step<2><<<blocks, 128, 0, s>>>(a); break;
-    default: k_chain_step<3><<<blocks, 128, 0, s>>>(a); break;
+    case 0: k_chain_view<0><<<g1, 128, 0, s>>>(a); k_chain_adam<0><<<blocks, 128, 0, s>>>(a); break;
+    case 1: k_chain_view<1><<<g1, 128, 0, s>>>(a); k_chain_adam<1><<<blocks, 128, 0, s>>>(a); break;
+    case 2: k_chain_view<2><<<g1, 128, 0, s>>>(a); k_chain_adam<2><<<blocks, 128, 0, s>>>(a); break;
+    default: k_chain_view<3><<<g1, 128, 0, s>>>(a); k_chain_adam<3><<<blocks, 128, 0, s>>>(a); break;
   }
 }
 

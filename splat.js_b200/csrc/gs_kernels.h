@@ -139,6 +139,10 @@ struct AdamHP {
   float b1, b2, eps, bc1, bc2, minLS, maxLS, maxLogit, reg, shLr;
 };
 
+// floats per (view, splat) chain result: 14 parameter gradients, gated
+// colour gradient (3), view direction (3)
+constexpr int VIEWGRAD_STRIDE = 20;
+
 struct ChainArgs {
   uint32_t n;
   int V;
@@ -146,7 +150,10 @@ struct ChainArgs {
   float* params;
   float* sh;
   int32_t* gradP;
-  const uint2* rect;        // V * n tile rectangles (x = 0xFFFFFFFF: not visible in that view)
+  const uint2* rect;
+  float* viewGrad;         // V * n * VIEWGRAD_STRIDE: per-(view, splat) chain results
+  uint32_t* visList;       // V * n: per view, indices of the visible splats
+  uint32_t* visCount;      // V counters, cleared before the step
   float anisoReg;
   int32_t* gradCam;
   float* gradF;            // optional readout (n * 16)

@@ -80,6 +80,8 @@ struct gs_trainer {
   uint32_t *counts = nullptr, *offsets = nullptr;
   float4* cullRecs = nullptr;
   uint4* itemRecs = nullptr;
+  float* viewGrad = nullptr;
+  uint32_t* visList = nullptr;
   uint4* itemSrc = nullptr;
   int32_t* gradP = nullptr;
   int32_t* diffGrid = nullptr;
@@ -381,6 +383,8 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   GS_AL(h->cullRecs, (size_t)B * cap);
   GS_AL(h->itemRecs, (size_t)B * cap * 2);
   GS_AL(h->itemSrc, (size_t)B * cap * 2);
+  GS_AL(h->viewGrad, (size_t)B * cap * VIEWGRAD_STRIDE);
+  GS_AL(h->visList, (size_t)B * cap);
   GS_AL(h->gradP, (size_t)B * cap * GP_STRIDE);
   // (tx+1)(ty+1) = tiles + tx + ty + 1 <= 3 * maxTiles + 1 for any view of at most maxTiles tiles
   GS_AL(h->diffGrid, (size_t)B * (3 * (size_t)h->maxTiles + 1));
@@ -576,6 +580,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   }
   cudaMemsetAsync(h->diffGrid, 0, (size_t)gridCells * 4, s);
   cudaMemsetAsync(h->small, 0, 2057 * 4, s);  // hist, tile counters, work counter
+  cudaMemsetAsync(h->small + 2062, 0, MAXB * 4, s);  // visible-item counters of the chain
   const uint64_t items = (uint64_t)sh.n * V;
 
   ProjectArgs pa{};
@@ -691,9 +696,9 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   if (cull) launch_ranges_from_keys(h->keys[passes & 1], totalEntries, totalTiles, h->ranges, s);
   // kernels: project, tile counts + finish, presort (histogram + passes),
   // entry counts, 3 scan kernels, entry keys, tile sort (histogram +
-  // passes), [ranges from keys], [work order: 3], raster, [chain + Adam]
+  // passes), [ranges from keys], [work order: 3], raster, [visible lists, chain per view, sum + Adam]
   h->lastLaunches = 3u + 1u + (uint32_t)pr.passes + 1u + 3u + 1u + 1u + (uint32_t)passes + (cull ? 1u : 0u) +
-                    (h->o.persistent ? 3u : 0u) + 1u + (sh.chain ? 1u : 0u);
+                    (h->o.persistent ? 3u : 0u) + 1u + (sh.chain ? 3u : 0u);
   const uint32_t* sortedIds = h->vals[passes & 1];
 
   const bool persistent = h->o.persistent != 0;
@@ -739,6 +744,9 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
     c.sh = h->K ? h->sh : nullptr;
     c.gradP = h->gradP;
     c.rect = h->rect;
+    c.viewGrad = h->viewGrad;
+    c.visList = h->visList;
+    c.visCount = h->small + 2062;
     c.anisoReg = h->o.anisoReg;
     c.gradCam = h->gradCam;
     c.gradF = sh.grads ? h->gradFOut : nullptr;
