@@ -213,22 +213,43 @@ __device__ __forceinline__ void chainOne(const DevCam& c, const float* P, const 
   dRGBo[0] = dRGB[0]; dRGBo[1] = dRGB[1]; dRGBo[2] = dRGB[2];
 }
 
-__device__ __forceinline__ void adamParam(const AdamHP& h, int slot, float& p, float g, float& m, float& v) {
-  const float lr = h.lr[slot];
-  if (lr == 0.0f) return;
-  if (!(fabsf(g) < 1e18f)) g = 0.0f;
-  if (slot == 13) {
-    const float sg = sigm(p);
-    g = g + h.reg * sg * (1.0f - sg);
-  }
-  m = h.b1 * m + (1.0f - h.b1) * g;
-  v = h.b2 * v + (1.0f - h.b2) * g * g;
-  const float mh = m / h.bc1, vh = v / h.bc2;
-  float pn = p - h.lr[slot] * mh / (sqrtf(vh) + h.eps);
-  if (slot >= 3 && slot <= 5) pn = clampf(pn, h.minLS, h.maxLS);
-  if (slot >= 10 && slot <= 13) pn = clampf(pn, -h.maxLogit, h.maxLogit);
-  p = pn;
+// Adam for one parameter slot (shaders.js:984-1036).  The slot's learning
+// rate, clamp and regulariser are the same for every element a thread
+// updates (a block's 128 threads cover the 16 slots eight times over), so
+// they are resolved once per thread: AdamSlot holds them in registers and
+// the per-element update is straight-line.  The opacity slot's regularised
+// gradient (sanitised, plus reg * s * (1 - s) of the opacity before the
+// update) is computed per splat beforehand and passed in as g.
+struct AdamSlot {
+  float lr, lo, hi;
+  bool live, clamp, opa;
+};
+__device__ __forceinline__ AdamSlot adam_slot(const AdamHP& h, int slot) {
+  AdamSlot r;
+  r.lr = h.lr[slot];
+  r.live = r.lr != 0.0f;
+  const bool ls = slot >= 3 && slot <= 5, lg = slot >= 10 && slot <= 13;
+  r.clamp = ls || lg;
+  r.lo = ls ? h.minLS : -h.maxLogit;
+  r.hi = ls ? h.maxLS : h.maxLogit;
+  r.opa = slot == 13;
+  return r;
 }
+struct AdamK {  // the step's Adam constants, read once per thread
+  float b1, b2, ob1, ob2, bc1, bc2, eps, reg, shLr;
+};
+__device__ __forceinline__ AdamK adam_k(const AdamHP& h) {
+  return AdamK{h.b1, h.b2, 1.0f - h.b1, 1.0f - h.b2, h.bc1, h.bc2, h.eps, h.reg, h.shLr};
+}
+// m, v and the parameter after one step; g already sanitised
+__device__ __forceinline__ float adam_update(const AdamK& k, float lr, float p, float g, float& m, float& v) {
+  m = k.b1 * m + k.ob1 * g;
+  v = k.b2 * v + k.ob2 * g * g;
+  const float mh = m / k.bc1, vh = v / k.bc2;
+  return p - lr * mh / (sqrtf(vh) + k.eps);
+}
+// the sanitising of shaders.js:990 (non-finite or huge gradients count as 0)
+__device__ __forceinline__ float adam_g(float g) { return fabsf(g) < 1e18f ? g : 0.0f; }
 
 #ifndef GS_CHAIN_MIN_BLOCKS
 #define GS_CHAIN_MIN_BLOCKS 4  // resident 128-thread blocks per SM the register allocation must allow (no spills)
@@ -361,6 +382,7 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
   constexpr uint32_t SHD = SHN > 0 ? SHN : 1;  // divisor (the SH loops are empty when SHN = 0)
   __shared__ float s_g[128 * GROW];
   __shared__ float s_sh[SHN > 0 ? 128 * SROW : 1];
+  __shared__ float s_opa[128];
   const uint32_t i0 = blockIdx.x * blockDim.x;
   const uint32_t i = i0 + threadIdx.x;
   const int t = threadIdx.x;
@@ -400,6 +422,10 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
     for (int k = 0; k < 14; ++k) s_g[t * GROW + k] = gFa[k];
     s_g[t * GROW + 14] = 0.0f;
     s_g[t * GROW + 15] = 0.0f;
+    if (a.doAdam && i < a.n) {  // the opacity slot's gradient as Adam sees it (shaders.js:990-995)
+      const float sg = sigm(a.params[(size_t)i * STRIDE + 13]);
+      s_opa[t] = adam_g(gFa[13]) + a.hp->reg * sg * (1.0f - sg);
+    }
 #pragma unroll
     for (int k = 0; k < SHN; ++k) s_sh[t * SROW + k] = shA[k];
   }
@@ -412,7 +438,7 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
     for (uint32_t e = t; e < nS; e += 128) a.shGrad[sBase + e] = s_sh[(e / SHD) * SROW + e % SHD];
   }
   if (!a.doAdam) return;
-  const AdamHP& h = *a.hp;
+  const AdamK k = adam_k(*a.hp);
   // four elements per thread in flight: loads first, then the updates
   constexpr uint32_t U = 4;
   {
@@ -420,19 +446,25 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
     float* __restrict__ Pm = a.m + pBase;
     float* __restrict__ Pv = a.v + pBase;
     const int slot = t % STRIDE;  // 128 is a multiple of the stride: one slot per thread
-    for (uint32_t e0 = t; e0 < nP; e0 += 128 * U) {
-      float p[U], m[U], vv[U];
+    const AdamSlot as = adam_slot(*a.hp, slot);
+    if (as.live) {  // a zero learning rate leaves the slot as it is (shaders.js:986)
+      for (uint32_t e0 = t; e0 < nP; e0 += 128 * U) {
+        float p[U], m[U], vv[U];
 #pragma unroll
-      for (uint32_t u = 0; u < U; ++u) {
-        const uint32_t e = e0 + 128 * u;
-        if (e < nP) { p[u] = Pp[e]; m[u] = Pm[e]; vv[u] = Pv[e]; }
-      }
+        for (uint32_t u = 0; u < U; ++u) {
+          const uint32_t e = e0 + 128 * u;
+          if (e < nP) { p[u] = Pp[e]; m[u] = Pm[e]; vv[u] = Pv[e]; }
+        }
 #pragma unroll
-      for (uint32_t u = 0; u < U; ++u) {
-        const uint32_t e = e0 + 128 * u;
-        if (e < nP) {
-          adamParam(h, slot, p[u], s_g[(e / STRIDE) * GROW + slot], m[u], vv[u]);
-          Pp[e] = p[u]; Pm[e] = m[u]; Pv[e] = vv[u];
+        for (uint32_t u = 0; u < U; ++u) {
+          const uint32_t e = e0 + 128 * u;
+          if (e < nP) {
+            const uint32_t row = e / STRIDE;
+            const float g = as.opa ? s_opa[row] : adam_g(s_g[row * GROW + slot]);
+            float pn = adam_update(k, as.lr, p[u], g, m[u], vv[u]);
+            if (as.clamp) pn = clampf(pn, as.lo, as.hi);
+            Pp[e] = pn; Pm[e] = m[u]; Pv[e] = vv[u];
+          }
         }
       }
     }
@@ -452,14 +484,11 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
       for (uint32_t u = 0; u < U; ++u) {
         const uint32_t e = e0 + 128 * u;
         if (e < nS) {
-          float g = s_sh[(e / SHD) * SROW + e % SHD];
-          if (!(fabsf(g) < 1e18f)) g = 0.0f;
-          const float mk = h.b1 * m[u] + (1.0f - h.b1) * g;
-          const float vk = h.b2 * vv[u] + (1.0f - h.b2) * g * g;
-          const float mh = mk / h.bc1, vh = vk / h.bc2;
-          Sm[e] = mk;
-          Sv[e] = vk;
-          Sw[e] = w[u] - h.shLr * mh / (sqrtf(vh) + h.eps);
+          const float g = adam_g(s_sh[(e / SHD) * SROW + e % SHD]);
+          const float wn = adam_update(k, k.shLr, w[u], g, m[u], vv[u]);
+          Sm[e] = m[u];
+          Sv[e] = vv[u];
+          Sw[e] = wn;
         }
       }
     }

@@ -23,6 +23,7 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import os
 import time
 
 import numpy as np
@@ -46,13 +47,30 @@ def parse(argv=None):
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--batch-depth", type=int, default=256, choices=[64, 128, 256])
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--hbm-gbs", type=float, default=6534.5, help="measured HBM copy bandwidth, GB/s")
+    ap.add_argument("--hbm-gbs", type=float, default=None,
+                    help="HBM copy bandwidth, GB/s (default: MEASURED_PEAKS.json's hbm_gbs at the repository root)")
     ap.add_argument("--profile-window", action="store_true")
     return ap.parse_args(argv)
 
 
+def measured_hbm_gbs(default: float = 6542.1) -> tuple[float, str]:
+    """The measured HBM copy bandwidth of MEASURED_PEAKS.json (repository
+    root) when the file is present, else the default (a copy-bandwidth
+    measurement on a B200 of the same pool)."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "..", "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json"
+    except (OSError, KeyError, ValueError):
+        return default, "default"
+
+
 def main(argv=None):
     a = parse(argv)
+    if a.hbm_gbs is None:
+        a.hbm_gbs, hbm_source = measured_hbm_gbs()
+    else:
+        hbm_source = "--hbm-gbs"
     n, V, W, H = a.splats, a.views, a.width, a.height
     K = scene.sh_rest_coefs(a.sh_degree)
     params, sh = scene.surface_scene(n, seed=a.seed, sh_deg=a.sh_degree, log_scale=(-5.0, 0.7),
@@ -128,7 +146,8 @@ def main(argv=None):
                                         resolution=f"{W}x{H}"),
                           step_ms=step_ms, views_per_s=V / step_ms * 1e3,
                           phases_ms=dict(zip(["project_bin", "sort", "raster", "chain_adam"], ph)),
-                          pairs=P, reference_entries=E, fp32_peak_tflops=peak.value, rates=rate,
+                          pairs=P, reference_entries=E, fp32_peak_tflops=peak.value,
+                          hbm_gbs=a.hbm_gbs, hbm_source=hbm_source, rates=rate,
                           roofline_frac=frac)))
 
 
