@@ -43,13 +43,13 @@ __device__ __forceinline__ void chainOne(const DevCam& c, const float* P, const 
   float gva = -p00, gvb = -(p01 + p10), gvc = -p11;
   // comp -> raw 2D covariance (shaders.js:779-788)
   const float detV = fmaxf(g.va * g.vc - g.vb * g.vb, 0.0f);
-  const float comp = sqrtf(fmaxf(detV / detVd, 0.0f));
+  const float comp = sqrt_nz(fmaxf(div_nz(detV, detVd), 0.0f));
   if (comp > 1e-4f) {
     const float gcomp = gp[5];
     const float denom = 2.0f * comp * detVd;
-    gva = gva + gcomp * (g.vc - comp * comp * cd) / denom;
-    gvc = gvc + gcomp * (g.va - comp * comp * ad) / denom;
-    gvb = gvb + gcomp * (2.0f * g.vb * (comp * comp - 1.0f)) / denom;
+    gva = gva + div_nz(gcomp * (g.vc - comp * comp * cd), denom);
+    gvc = gvc + div_nz(gcomp * (g.va - comp * comp * ad), denom);
+    gvb = gvb + div_nz(gcomp * (2.0f * g.vb * (comp * comp - 1.0f)), denom);
   }
   // V = T Sigma T^T backward (shaders.js:790-810)
   const float h11 = gva, h12 = 0.5f * gvb, h22 = gvc;
@@ -168,7 +168,7 @@ __device__ __forceinline__ void chainOne(const DevCam& c, const float* P, const 
   const float ql = fmaxf(sqrtf(P[6] * P[6] + P[7] * P[7] + P[8] * P[8] + P[9] * P[9]), 1e-6f);
   const float qd = g.q[0] * gq[0] + g.q[1] * gq[1] + g.q[2] * gq[2] + g.q[3] * gq[3];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) gF[6 + k] = (gq[k] - g.q[k] * qd) / ql;
+  for (int k = 0; k < 4; ++k) gF[6 + k] = div_nz(gq[k] - g.q[k] * qd, ql);
   // colour: DC sigmoid chain + SH bands (+ position via view dir) (shaders.js:906-947)
   const float sCol[3] = {sigm(P[10]), sigm(P[11]), sigm(P[12])};
   float dRGB[3] = {gp[7], gp[8], gp[9]};
@@ -205,7 +205,7 @@ __device__ __forceinline__ void chainOne(const DevCam& c, const float* P, const 
       }
     const float vg = dot3(vd, gv);
 #pragma unroll
-    for (int j = 0; j < 3; ++j) gF[j] = gF[j] + (gv[j] - vd[j] * vg) / ulen;
+    for (int j = 0; j < 3; ++j) gF[j] = gF[j] + div_nz(gv[j] - vd[j] * vg, ulen);
   }
 #pragma unroll
   for (int j = 0; j < 3; ++j) gF[10 + j] = dRGB[j] * sCol[j] * (1.0f - sCol[j]);
@@ -245,8 +245,8 @@ __device__ __forceinline__ AdamK adam_k(const AdamHP& h) {
 __device__ __forceinline__ float adam_update(const AdamK& k, float lr, float p, float g, float& m, float& v) {
   m = k.b1 * m + k.ob1 * g;
   v = k.b2 * v + k.ob2 * g * g;
-  const float mh = m / k.bc1, vh = v / k.bc2;
-  return p - lr * mh / (sqrtf(vh) + k.eps);
+  const float mh = div_nz(m, k.bc1), vh = div_nz(v, k.bc2);
+  return p - div_nz(lr * mh, sqrt_nz(vh) + k.eps);
 }
 // the sanitising of shaders.js:990 (non-finite or huge gradients count as 0)
 __device__ __forceinline__ float adam_g(float g) { return fabsf(g) < 1e18f ? g : 0.0f; }

@@ -289,6 +289,30 @@ __device__ __forceinline__ double gsin_d(double x) {
 }
 
 __device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+// x / d (IEEE, div.rn.f32) with a zero numerator answered without dividing:
+// +-0 / d = +-0 exactly for every d > 0, +inf included; other d divide as
+// written.  Zero numerators are common in the per-splat passes (parameters
+// whose gradient history is all zero, splats that composited nowhere), and
+// the compiled division takes its out-of-line path for them: measured on the
+// Adam pass, every division and square root branched out of line in about
+// three warp-instances of four.  The division is written as a PTX
+// instruction so that the guard's select stays on its operand (as a C
+// expression the compiler may fold the select into the quotient and divide
+// the zero after all).  The result is bit-identical to x / d.
+__device__ __forceinline__ float div_nz(float x, float d) {
+  const bool z = x == 0.0f && d > 0.0f;
+  float q;
+  asm("div.rn.f32 %0, %1, %2;" : "=f"(q) : "f"(z ? 1.0f : x), "f"(d));
+  return z ? x : q;
+}
+// sqrt(x) (IEEE, sqrt.rn.f32) with zero answered without the root:
+// sqrt(+-0) = +-0.
+__device__ __forceinline__ float sqrt_nz(float x) {
+  const bool z = x == 0.0f;
+  float r;
+  asm("sqrt.rn.f32 %0, %1;" : "=f"(r) : "f"(z ? 1.0f : x));
+  return z ? x : r;
+}
 // 1 / (1 + exp(-clamp(x, -9, 9)))
 __device__ __forceinline__ float sigm(float x) { return 1.0f / (1.0f + gexp(-clampf(x, -9.0f, 9.0f))); }
 // i32(clamp(v * scale, -1e9, 1e9)) with WGSL's truncating cast (shaders.js:529-541)
