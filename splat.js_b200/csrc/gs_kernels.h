@@ -110,6 +110,8 @@ struct RadixSortArgs {
   unsigned histGrid, sweepGrid;
   uint32_t* nKept;          // non-null (32-bit keys): all-ones keys are dropped in the first pass and the
                             // kept count lands here (zero before the call); later passes sort only those
+  uint32_t orPasses;        // 32-bit keys, bit p: pass p ranks its digits with the OR form (digits spread
+                            // across a warp: tile ids, the low bytes of depths)
 };
 
 struct RasterArgs {

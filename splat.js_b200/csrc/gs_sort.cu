@@ -189,7 +189,14 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   return m;
 }
 
-template <typename KT, bool DROP = false>
+// Digit ranking inside a warp (stable: items in order, lanes in order).
+// Ballot form: eight votes on the digit's bits intersect to the lanes that
+// share it.  OR form (ORM): every lane sets its bit in a shared-memory word
+// of its digit and reads the word back, so one shared atomic and two loads
+// replace the eight votes and their bit tests; lanes with equal digits hit
+// the same word, so it pays where a warp's digits are spread (tile ids) and
+// not where most of them are equal (the top bytes of depths).
+template <typename KT, bool DROP = false, bool ORM = false>
 #ifndef GS_SORT_MIN_BLOCKS
 #define GS_SORT_MIN_BLOCKS 3  // resident blocks per SM the register allocation must allow
 #endif
@@ -207,6 +214,7 @@ __global__ void __launch_bounds__(RS_THREADS, GS_SORT_MIN_BLOCKS) k_onesweep(One
   __shared__ uint32_t s_dbase[256];     // exclusive scan of the pass histogram
   __shared__ uint32_t s_warp[33];
   __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_match[ORM ? RS_WARPS : 1][256];  // OR form: per warp, lanes holding each digit
 
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const uint32_t N = *a.nItems;
@@ -214,6 +222,10 @@ __global__ void __launch_bounds__(RS_THREADS, GS_SORT_MIN_BLOCKS) k_onesweep(One
   const uint32_t tag = a.epoch[0] * RS_MAX_PASSES + (uint32_t)a.pass + 1u;
   const int shift = 8 * a.pass;
 
+  if (ORM) {  // the words return to zero after every item, so once per launch
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; ++w) s_match[ORM ? w : 0][tid] = 0u;
+  }
   // global digit bases: exclusive scan of this pass's histogram (256 threads)
   {
     const uint32_t hv = a.hist[a.pass * 256 + tid];
@@ -268,26 +280,50 @@ __global__ void __launch_bounds__(RS_THREADS, GS_SORT_MIN_BLOCKS) k_onesweep(One
     // rank within the warp, items in order, lanes in order
     uint32_t rank[RS_ITEMS];
     const uint32_t ltm = lanemask_lt();
+    if (ORM) {
+      uint32_t* wm = s_match[ORM ? wid : 0];
 #pragma unroll
-    for (int j = 0; j < RS_ITEMS; ++j) {
-      const bool valid = dig[j] < 0x100u;
-      uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
+      for (int j = 0; j < RS_ITEMS; ++j) {
+        const bool valid = dig[j] < 0x100u;
+        if (valid) atomicOr(&wm[dig[j]], 1u << lane);
+        __syncwarp();
+        uint32_t peers = 0, pre = 0;
+        if (valid) { peers = wm[dig[j]]; pre = s_whist[wid][dig[j]]; }
+        __syncwarp();
+        if (valid) {
+          const uint32_t below = __popc(peers & ltm);
+          rank[j] = pre + below;
+          if (below == 0) {  // the digit's first lane advances its count and clears the word
+            s_whist[wid][dig[j]] = pre + __popc(peers);
+            wm[dig[j]] = 0u;
+          }
+        } else {
+          rank[j] = 0;
+        }
+        __syncwarp();
+      }
+    } else {
 #pragma unroll
-      for (int b = 0; b < 8; ++b) {
-        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, (dig[j] >> b) & 1u);
-        peers &= ((dig[j] >> b) & 1u) ? bal : ~bal;
+      for (int j = 0; j < RS_ITEMS; ++j) {
+        const bool valid = dig[j] < 0x100u;
+        uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, (dig[j] >> b) & 1u);
+          peers &= ((dig[j] >> b) & 1u) ? bal : ~bal;
+        }
+        uint32_t pre = 0;
+        if (valid) pre = s_whist[wid][dig[j]];
+        __syncwarp();
+        if (valid) {
+          const uint32_t below = __popc(peers & ltm);
+          rank[j] = pre + below;
+          if (below == 0) s_whist[wid][dig[j]] = pre + __popc(peers);
+        } else {
+          rank[j] = 0;
+        }
+        __syncwarp();
       }
-      uint32_t pre = 0;
-      if (valid) pre = s_whist[wid][dig[j]];
-      __syncwarp();
-      if (valid) {
-        const uint32_t below = __popc(peers & ltm);
-        rank[j] = pre + below;
-        if (below == 0) s_whist[wid][dig[j]] = pre + __popc(peers);
-      } else {
-        rank[j] = 0;
-      }
-      __syncwarp();
     }
     __syncthreads();
 
@@ -433,9 +469,17 @@ int onesweep_grid(int device) {
                        (int)rs_dyn_smem<uint32_t>());
   cudaFuncSetAttribute(k_onesweep<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)rs_dyn_smem<uint64_t>());
+  cudaFuncSetAttribute(k_onesweep<uint32_t, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)rs_dyn_smem<uint32_t>());
+  cudaFuncSetAttribute(k_onesweep<uint32_t, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)rs_dyn_smem<uint32_t>());
+  int perOr = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_onesweep<uint32_t>, RS_THREADS, rs_dyn_smem<uint32_t>());
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per64, k_onesweep<uint64_t>, RS_THREADS, rs_dyn_smem<uint64_t>());
-  int perSm = per32 < per64 ? per32 : per64;  // one grid size that is fully resident for both key widths
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perOr, k_onesweep<uint32_t, false, true>, RS_THREADS,
+                                                rs_dyn_smem<uint32_t>());
+  int perSm = per32 < per64 ? per32 : per64;  // one grid size that is fully resident for every form
+  if (perOr < perSm) perSm = perOr;
   if (perSm < 1) perSm = 1;
   return sms * perSm;
 }
@@ -473,7 +517,12 @@ static void radix_sort_t(const RadixSortArgs& a, cudaStream_t s) {
     o.epoch = a.epoch;
     o.pass = p;
     o.spinLimit = LOOKBACK_SPIN_LIMIT;
-    if (o.dropAllOnes) k_onesweep<KT, true><<<a.sweepGrid, RS_THREADS, rs_dyn_smem<KT>(), s>>>(o);
+    const bool orForm = sizeof(KT) == 4 && ((a.orPasses >> p) & 1u);
+    if (o.dropAllOnes && orForm)
+      k_onesweep<uint32_t, true, true><<<a.sweepGrid, RS_THREADS, rs_dyn_smem<uint32_t>(), s>>>(o);
+    else if (o.dropAllOnes) k_onesweep<KT, true><<<a.sweepGrid, RS_THREADS, rs_dyn_smem<KT>(), s>>>(o);
+    else if (orForm)
+      k_onesweep<uint32_t, false, true><<<a.sweepGrid, RS_THREADS, rs_dyn_smem<uint32_t>(), s>>>(o);
     else k_onesweep<KT><<<a.sweepGrid, RS_THREADS, rs_dyn_smem<KT>(), s>>>(o);
   }
 }

@@ -636,6 +636,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   pr.epoch = epoch;
   pr.passes = 4;
   pr.keepKeys = false;
+  pr.orPasses = 0x7u;  // depth bytes 0-2 spread across a warp; the top byte (sign, exponent) is shared
   pr.histGrid = (unsigned)h->histGrid;
   pr.sweepGrid = (unsigned)h->sweepGrid;
   // culled items (all-ones keys) leave the presort: only the visible ones
@@ -689,6 +690,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   ra.epoch = epoch;
   ra.passes = passes;
   ra.keepKeys = cull;  // culled lists take their tile ranges from the sorted keys
+  ra.orPasses = 0xFFu;  // tile ids: every byte spread across a warp
   ra.histGrid = (unsigned)h->histGrid;
   ra.sweepGrid = (unsigned)h->sweepGrid;
   launch_radix_sort(ra, s);
