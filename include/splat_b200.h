@@ -190,7 +190,10 @@ GS_API int gs_read_cam_grads(gs_trainer* h, int32_t* out, int32_t reset);
 /* refine(rng) (trainer.js:666-794): dead/donor classification, donor order
  * and the parameter writes run on the device; only rng() draws are made on
  * the host, in the reference's order.  gs_options.donorSampling = 1 picks
- * clone donors by opacity weight from the same draws. */
+ * clone donors by opacity weight from the same draws.  rng = NULL (the
+ * reference's default, Math.random) draws from the handle's own generator,
+ * xorshift128+ with a fixed starting state that continues across calls
+ * (ctx unused): reproducible, and no call per draw into the caller. */
 GS_API int gs_refine(gs_trainer* h, gs_rng_fn rng, void* ctx, gs_refine_result* out);
 /* device.queue.onSubmittedWorkDone() (session.js:520, 542): waits for the stream. */
 GS_API int gs_sync(gs_trainer* h);

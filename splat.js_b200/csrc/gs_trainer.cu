@@ -63,6 +63,7 @@ struct gs_trainer {
   // ---- host state (GSTrainer fields) ----
   uint32_t n = 0, cap = 0, K = 0, ncams = 0, iter = 0, horizon = 60000, growLimit = 0;
   uint64_t pixelsSeen = 0, entriesCap = 12000000ull, overflowTiles = 0;
+  uint64_t rngState[2] = {0x2BD3AB5E4C1D2B3Bull, 0x9C3F7A1E0D5B6C47ull};  // built-in refine generator
   double sceneRadius = 1.0;
   double basePosLr = 0.0;
   float lrs[16] = {};
@@ -157,6 +158,24 @@ struct gs_trainer {
 static int fail(gs_trainer* h, int code, const std::string& msg) {
   h->err = msg;
   return code;
+}
+
+// refine()'s default rng (the reference defaults to Math.random, a native
+// generator): xorshift128+ (S. Vigna, "Further scramblings of Marsaglia's
+// xorshift generators", J. Comput. Appl. Math. 315, 2017; shifts 23, 18, 5),
+// 53 high bits of each output as a double in [0, 1).  The state lives in the
+// handle, starts from the same two words for every handle and continues
+// across refine calls, so a run is reproducible; the draws cost nanoseconds
+// instead of a call into the caller's language per draw.
+static double builtin_rng(void* ctx) {
+  uint64_t* st = static_cast<gs_trainer*>(ctx)->rngState;
+  uint64_t s1 = st[0];
+  const uint64_t s0 = st[1];
+  const uint64_t out = s0 + s1;
+  st[0] = s0;
+  s1 ^= s1 << 23;
+  st[1] = s1 ^ s0 ^ (s1 >> 18) ^ (s0 >> 5);
+  return (double)(out >> 11) * 0x1.0p-53;
 }
 
 template <class T>
@@ -1300,7 +1319,8 @@ int gs_profile_read(gs_trainer* h, double ms[4], uint32_t launches[4]) {
 // counts and makes the rng() draws in the reference's order (the draws
 // decide which donor each spawn copies, so they are inherently sequential).
 int gs_refine(gs_trainer* h, gs_rng_fn rng, void* ctx, gs_refine_result* out) {
-  if (!h || !rng || !out) return GS_E_INVALID;
+  if (!h || !out) return GS_E_INVALID;
+  if (!rng) { rng = builtin_rng; ctx = h; }
   if (!h->ready) return fail(h, GS_E_INVALID, "setup() first");
   cudaSetDevice(h->device);
   cudaStream_t s = h->stream;

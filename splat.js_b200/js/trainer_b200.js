@@ -131,8 +131,10 @@ export class GSTrainer {
     return this.renderView(m, target, 0, m.offset);
   }
 
-  // refine(rng) (trainer.js:666-794); rng must not call back into this trainer
-  async refine(rng = Math.random) {
+  // refine(rng) (trainer.js:666-794); rng must not call back into this trainer.
+  // Without an rng the library's own generator draws (the reference's default
+  // is Math.random): no call into JavaScript per draw.
+  async refine(rng) {
     addon.setGrowLimit(this.h, this.growLimit || 0);
     return addon.refine(this.h, rng);
   }

@@ -602,20 +602,25 @@ static double call_rng(void* ctx) {
 }
 
 /* refine(h, rng) -> {moved, grown, n, maxTile, overflow} or {moved: 0, grown: 0, n}
- * (the donors < 16 early return, trainer.js:695) */
+ * (the donors < 16 early return, trainer.js:695); rng undefined or null: the
+ * library's own generator draws, with no call into JavaScript per draw */
 static napi_value Refine(napi_env env, napi_callback_info info) {
   size_t argc = 2;
   napi_value argv[2];
   NAPI_OK(env, napi_get_cb_info(env, info, &argc, argv, NULL, NULL));
   Handle* H = arg_handle(env, argv[0]);
   if (!H) return NULL;
-  napi_valuetype t;
-  NAPI_OK(env, napi_typeof(env, argv[1], &t));
-  if (t != napi_function) { napi_throw_error(env, NULL, "refine: rng must be a function"); return NULL; }
-  RngCtx ctx = {env, argv[1], 0};
+  napi_valuetype t = napi_undefined;
+  if (argc > 1) NAPI_OK(env, napi_typeof(env, argv[1], &t));
+  const bool own = t == napi_undefined || t == napi_null;  // the library's generator (no JS call per draw)
+  if (!own && t != napi_function) {
+    napi_throw_error(env, NULL, "refine: rng must be a function or undefined");
+    return NULL;
+  }
+  RngCtx ctx = {env, own ? NULL : argv[1], 0};
   gs_refine_result r;
   pthread_mutex_lock(&H->mu);
-  const int rc = gs_refine(H->h, call_rng, &ctx, &r);
+  const int rc = own ? gs_refine(H->h, NULL, NULL, &r) : gs_refine(H->h, call_rng, &ctx, &r);
   pthread_mutex_unlock(&H->mu);
   bool pending = false;
   napi_is_exception_pending(env, &pending);

@@ -8,7 +8,9 @@ Defaults are config 4: 2,000,000 splats of the seeded surface scene at SH
 degree 3 with a fifth of them fine (log-scale N(-7, 0.5)), four 1920x1080
 ring views per step (cameras spread over a 24-camera ring, rotating every
 step), 2000 steps starting at iteration 3000 (every SH band active), refine
-every 100 steps with opacity-weighted clone donors, a seeded rng() and 10%
+every 100 steps with opacity-weighted clone donors, the library's own
+reproducible generator as rng() (--rng lcg: a seeded LCG called from Python
+per draw, as a caller-supplied rng is) and 10%
 splat headroom (maxSplats = 1.1 n, so growth runs until the headroom is
 used and relocation every time).  Targets are the scene rendered from a
 perturbed copy.  Prints one JSON line: wall time of the whole schedule
@@ -60,6 +62,9 @@ def parse(argv=None):
     ap.add_argument("--donor-sampling", type=int, default=1, choices=[0, 1])
     ap.add_argument("--batch-depth", type=int, default=256, choices=[64, 128, 256])
     ap.add_argument("--seed", type=int, default=4)
+    ap.add_argument("--rng", choices=["own", "lcg"], default="own",
+                    help="refine's rng(): the library's own generator (the reference's default is Math.random), "
+                         "or a seeded LCG in Python called once per draw")
     ap.add_argument("--profile-window", action="store_true")
     return ap.parse_args(argv)
 
@@ -90,7 +95,7 @@ def main(argv=None):
     def batch(k):
         return [(k + j * stride) % a.cams for j in range(V)]
 
-    rng = lcg(a.seed)
+    rng = lcg(a.seed) if a.rng == "lcg" else None
     if a.profile_window:
         import torch
         for k in range(3):
@@ -135,7 +140,7 @@ def main(argv=None):
         workload=dict(splats=n, max_splats=cap, sh_degree=a.sh_degree, fine_frac=a.fine_frac, views_per_step=V,
                       resolution=f"{W}x{H}", steps=a.steps, refine_every=a.refine_every,
                       donor_sampling="opacity-weighted" if a.donor_sampling else "uniform (reference)",
-                      iteration_start=3000),
+                      iteration_start=3000, rng="library generator" if a.rng == "own" else "Python LCG per draw"),
         wall_s=wall, steps_per_s=a.steps / wall, views_per_s=a.steps * V / wall,
         refines=refines, refine_s=refine_s, refine_ms_each=refine_s / max(1, refines) * 1e3,
         moved=moved, grown=grown, final_splats=t.n,

@@ -352,8 +352,11 @@ class GSTrainer:
 
     # ---- refinement (trainer.js:666-794) ----
     def refine(self, rng=None):
-        rng = rng or random.random
-        cb = N.RNG_FN(lambda _ctx: float(rng()))
+        """refine(rng) (trainer.js:666-794).  rng: a callable returning floats
+        in [0, 1), drawn in the reference's order; None draws from the
+        library's own generator (the reference's default is Math.random), with
+        no Python call per draw."""
+        cb = N.RNG_FN(lambda _ctx: float(rng())) if rng is not None else N.RNG_FN()  # NULL: own generator
         out = N.GsRefineResult()
         gl = int(self.growLimit or 0)
         N.check(N.lib().gs_set_grow_limit(self._h, gl), self._h)

@@ -21,6 +21,23 @@ def lcg(seed: int):
     return rnd
 
 
+def xorshift128p(s0: int = 0x2BD3AB5E4C1D2B3B, s1: int = 0x9C3F7A1E0D5B6C47):
+    """The library's own refine() generator, restated: xorshift128+ (Vigna
+    2017, shifts 23, 18, 5) from the handle's fixed starting state, the 53
+    high bits of each output as a double in [0, 1)."""
+    M = (1 << 64) - 1
+    st = [s0, s1]
+
+    def rnd():
+        a, b = st
+        out = (a + b) & M
+        st[0] = b
+        a = (a ^ (a << 23)) & M
+        st[1] = a ^ b ^ (a >> 18) ^ (b >> 5)
+        return (out >> 11) * 2.0 ** -53
+    return rnd
+
+
 def gradcheck_params(n=160):
     rnd = lcg(123456789)
     data = np.zeros(n * 16, np.float32)

@@ -7,7 +7,8 @@ trainer.js:666-794) every 100 steps.  Here the same pattern runs at a
 reduced size so the oracle keeps up: 30k splats, four 320x180 ring views,
 refine every 4 steps for three cycles (relocation every cycle, growth into
 the headroom), and every parameter, Adam moment and SH coefficient is
-compared after each cycle.  The schedule at full size is measured by
+compared after each cycle, with the caller's rng and with the library's own
+generator (refine() without an rng).  The schedule at full size is measured by
 ``python -m splat_b200.schedule``."""
 import numpy as np
 import pytest
@@ -20,8 +21,11 @@ from test_gpu_parity import assert_bits, make, oracle_adam, oracle_cam, oracle_o
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("donorSampling", [0, 1])
-def test_refine_cycles_bitexact(donorSampling):
+@pytest.mark.parametrize("donorSampling,rng", [(0, "caller"), (1, "caller"), (1, "own")])
+def test_refine_cycles_bitexact(donorSampling, rng):
+    """rng "caller": a seeded LCG passed to refine() (one call per draw);
+    "own": refine() without an rng draws from the library's generator, which
+    the oracle replays from its restatement."""
     n, cap, K, W, H = 30_000, 42_000, 15, 320, 180
     params, sh = scene.surface_scene(n, seed=14, sh_deg=3, log_scale=(-3.5, 0.6), fine_frac=0.2)
     P0 = params.reshape(-1, 16)
@@ -43,7 +47,10 @@ def test_refine_cycles_bitexact(donorSampling):
     M, V = np.zeros(cap * 16, np.float32), np.zeros(cap * 16, np.float32)
     SM, SV = np.zeros(cap * 3 * K, np.float32), np.zeros(cap * 3 * K, np.float32)
     nn, it = n, 3000
-    rng_gpu, rng_cpu = rigs.lcg(77 + donorSampling), rigs.lcg(77 + donorSampling)
+    if rng == "caller":
+        rng_gpu, rng_cpu = rigs.lcg(77 + donorSampling), rigs.lcg(77 + donorSampling)
+    else:
+        rng_gpu, rng_cpu = None, rigs.xorshift128p()
     moved = grown = 0
     for cycle in range(3):
         for _ in range(4):
