@@ -437,8 +437,12 @@ def run_ours(args):
                                       "read": "gs_read_stats each step (one host sync per step)"},
                 "gpu_launches": None,
                 "phases_ms_per_step": phase,
+                "steps_per_s": args.steps / (batch_ms * 1e-3),
                 "pairs_per_step": pairs_per_launch,
                 "pairs_executed_per_step": pairs_exec,
+                # splat-pixel evaluations/s: the reference's pixel-entry pairs P of a step over its time
+                "splat_pixel_evals_per_s": pairs_per_launch / (batch_ms * 1e-3 / args.steps)
+                if pairs_per_launch else None,
                 "roofline": {"bound": "fp32", "kernel": "raster (fused forward + loss + backward)",
                              "bound_note": "FP32 CUDA-core (issue) bound: no tensor-core or HBM bound applies; "
                                            "the peak is this GPU's measured FFMA throughput",
