@@ -321,10 +321,13 @@ def run_ours(args):
     s_host = np.ascontiguousarray(sh, np.float32)
 
     def restore():
-        # every timed segment starts from the same model (the steps train it,
-        # and the splats' footprints, hence the work, drift as they do)
+        # every timed segment starts from the same trainer state: the
+        # generator's parameters and SH, zero Adam moments (as setup leaves
+        # them) and iteration 2000 (the steps train the model, and the
+        # splats' footprints, hence the work, drift as they do)
         N.check(L.gs_write_gaussians(h, p_host.ctypes.data_as(C.POINTER(C.c_float)),
                                      s_host.ctypes.data_as(C.POINTER(C.c_float)), n), h)
+        N.check(L.gs_reset_moments(h), h)
         t.iter = 2000
 
     restore()

@@ -169,6 +169,10 @@ GS_API int gs_read_gaussians(gs_trainer* h, float* params, float* sh, uint32_t* 
 /* Overwrite the first n splats' parameters / SH (the parameter pokes of
  * gradcheck.js:320-323; either pointer may be NULL). */
 GS_API int gs_write_gaussians(gs_trainer* h, const float* params, const float* sh, uint32_t n);
+/* No reference counterpart: zeroes the Adam and SH-Adam moments of every
+ * slot, as setup() does (trainer.js:100-355), so a model written with
+ * gs_write_gaussians trains from the same optimiser state as a fresh setup. */
+GS_API int gs_reset_moments(gs_trainer* h);
 /* Adam moments (for refine parity checks): m, v n*16; shM, shV n*3K. */
 GS_API int gs_read_moments(gs_trainer* h, float* m, float* v, float* shM, float* shV);
 

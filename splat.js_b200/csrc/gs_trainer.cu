@@ -1014,6 +1014,21 @@ int gs_write_gaussians(gs_trainer* h, const float* params, const float* sh, uint
   return GS_OK;
 }
 
+int gs_reset_moments(gs_trainer* h) {
+  if (!h) return GS_E_INVALID;
+  if (!h->ready) return fail(h, GS_E_INVALID, "setup() first");
+  cudaSetDevice(h->device);
+  const size_t pb = (size_t)h->cap * 64, sb = (size_t)h->cap * 3 * h->K * 4;
+  GS_CK(cudaMemsetAsync(h->m, 0, pb, h->stream));
+  GS_CK(cudaMemsetAsync(h->v, 0, pb, h->stream));
+  if (sb) {
+    GS_CK(cudaMemsetAsync(h->shM, 0, sb, h->stream));
+    GS_CK(cudaMemsetAsync(h->shV, 0, sb, h->stream));
+  }
+  GS_CK(cudaStreamSynchronize(h->stream));
+  return GS_OK;
+}
+
 int gs_read_moments(gs_trainer* h, float* m, float* v, float* shM, float* shV) {
   if (!h) return GS_E_INVALID;
   if (!h->ready) return fail(h, GS_E_INVALID, "setup() first");

@@ -98,6 +98,7 @@ def lib():
                                     u64p]),
         "gs_write_gaussians": (C.c_int, [H, f32p, f32p, C.c_uint32]),
         "gs_read_moments": (C.c_int, [H, f32p, f32p, f32p, f32p]),
+        "gs_reset_moments": (C.c_int, [H]),
         "gs_render": (C.c_int, [H, P(GsCamera), C.c_int32, C.c_uint32, f32p]),
         "gs_eval_pass": (C.c_int, [H, C.c_uint32, P(GsCamera), u32p, i32p]),
         "gs_grad_pass": (C.c_int, [H, C.c_uint32, f32p, f32p, u32p]),

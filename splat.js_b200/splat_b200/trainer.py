@@ -243,6 +243,11 @@ class GSTrainer:
         s = None if sh is None else np.ascontiguousarray(sh, np.float32)
         N.check(N.lib().gs_write_gaussians(self._h, N.ptr(d), N.ptr(s), n), self._h)
 
+    def resetMoments(self):
+        """Zero the Adam and SH-Adam moments, as setup() does (no reference
+        counterpart): with writeGaussians, restarts training from a model."""
+        N.check(N.lib().gs_reset_moments(self._h), self._h)
+
     def readMoments(self):
         n, k3 = self.n, 3 * self.shK
         m = np.zeros(n * STRIDE, np.float32)

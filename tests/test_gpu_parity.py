@@ -954,3 +954,68 @@ def test_training_fits_a_rendered_target():
     g = t.readGaussians()
     assert np.isfinite(g["data"]).all() and np.isfinite(g["sh"]).all()
     assert losses[-1] < 0.8 * losses[0], losses
+
+
+@pytest.mark.parametrize("deg", [0, 1, 2, 3])
+def test_training_steps_every_sh_degree(deg):
+    """Two batched steps over two views at each SH degree the reference
+    supports (shDeg 0-3: K = 0, 3, 8, 15 rest coefficients per channel):
+    every degree's projection, chain and Adam instantiation against the
+    oracle, parameters, SH and all four moment buffers bit for bit."""
+    n = 8000
+    K = (deg + 1) ** 2 - 1
+    params, sh = scene.surface_scene(n, seed=20 + deg, sh_deg=deg, log_scale=(-3.5, 0.5))
+    cams = scene.ring_cameras(2, 4.0, 0.5, 160, 96, phase=0.2)
+    rgbs = [scene.uniform_target(160, 96, seed=40 + k) for k in range(2)]
+    t, targets, metas = make(params, sh, cams, rgbs, dict(shDeg=deg, maxBatch=2), radius=2.0)
+    t.iter = 1000 * deg  # every band of this degree active
+    o = oracle_opts(dict(shDeg=deg))
+    p, s = params.copy(), sh.copy()
+    m = np.zeros(n * 16, np.float32)
+    vv = np.zeros(n * 16, np.float32)
+    sm = np.zeros(max(1, n * 3 * K), np.float32)[:n * 3 * K]
+    sv = np.zeros(max(1, n * 3 * K), np.float32)[:n * 3 * K]
+    for k in range(2):
+        t.stepBatch([0, 1])
+        it = 1000 * deg + k + 1
+        ocams = [oracle_cam(metas[v], v, 2, deg) for v in range(2)]
+        O.step(o, ocams, oracle_adam(t, it, 2.0), p, s, targets, m, vv, sm, sv, n)
+        g = t.readGaussians()
+        assert_bits(g["data"], p, f"params after step {k + 1} at SH degree {deg}")
+        if K:
+            assert_bits(g["sh"], s, f"SH after step {k + 1} at SH degree {deg}")
+    gm, gv, gsm, gsv = t.readMoments()
+    assert_bits(gm, m, "Adam m")
+    assert_bits(gv, vv, "Adam v")
+    if K:
+        assert_bits(gsm, sm, "SH-Adam m")
+        assert_bits(gsv, sv, "SH-Adam v")
+
+
+def test_sixteen_view_batch_bitexact():
+    """A batch at its limit of 16 views (uneven sizes, one persistent
+    (view, tile) queue): one optimiser step against the oracle's batched
+    step, parameters and SH bit for bit."""
+    n = 6000
+    params, sh = scene.surface_scene(n, seed=31, sh_deg=2, log_scale=(-3.5, 0.5))
+    sizes = [(96, 64), (128, 72), (160, 96), (200, 120)]
+    cams, rgbs = [], []
+    for k in range(16):
+        w, h = sizes[k % 4]
+        cams.append(scene.ring_cameras(16, 4.0, 0.5, w, h, phase=0.1)[k])
+        rgbs.append(scene.uniform_target(w, h, seed=70 + k))
+    t, targets, metas = make(params, sh, cams, rgbs, dict(shDeg=2, maxBatch=16), radius=2.0)
+    t.iter = 2000
+    o = oracle_opts(dict(shDeg=2))
+    K = 8
+    p, s = params.copy(), sh.copy()
+    m = np.zeros(n * 16, np.float32)
+    vv = np.zeros(n * 16, np.float32)
+    sm = np.zeros(n * 3 * K, np.float32)
+    sv = np.zeros(n * 3 * K, np.float32)
+    t.stepBatch(list(range(16)))
+    ocams = [oracle_cam(metas[v], v, 16, 2) for v in range(16)]
+    O.step(o, ocams, oracle_adam(t, 2001, 2.0), p, s, targets, m, vv, sm, sv, n)
+    g = t.readGaussians()
+    assert_bits(g["data"], p, "params after a 16-view step")
+    assert_bits(g["sh"], s, "SH after a 16-view step")
