@@ -439,8 +439,11 @@ __global__ void __launch_bounds__(128) k_chain_adam(ChainArgs a) {
   }
   if (!a.doAdam) return;
   const AdamK k = adam_k(*a.hp);
-  // four elements per thread in flight: loads first, then the updates
-  constexpr uint32_t U = 4;
+  // U elements per thread in flight: loads first, then the updates.  At SH
+  // degree 3 the summing phase above already sets the register count (96),
+  // so six in flight cost no occupancy there (measured -10 % on the pass;
+  // ptxas spills 4 bytes); at the lower degrees more than four would.
+  constexpr uint32_t U = DEG == 3 ? 6 : 4;
   {
     float* __restrict__ Pp = a.params + pBase;
     float* __restrict__ Pm = a.m + pBase;
