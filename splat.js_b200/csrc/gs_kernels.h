@@ -8,6 +8,13 @@
 
 namespace gs {
 
+// The projection's rectangle adds go to one of GRID_COPIES copies of the
+// difference grid (by splat index), summed when the counts are read: every
+// splat of a tile adds to the same four corner cells, and spreading those
+// atomics over copies shortens the queues on the busiest cells.  Integer
+// sums: the counts do not depend on the split.
+constexpr uint32_t GRID_COPIES = 4;
+
 struct ProjectArgs {
   const float* params;     // n * 16
   const float* sh;         // n * 3K (channel-major) or null
@@ -20,8 +27,9 @@ struct ProjectArgs {
   uint32_t* pkeys;         // V * n presort keys: depth bits (all ones when culled)
   uint32_t* pvals;         // V * n presort values: slot = view * n + splat
   uint2* rect;             // V * n
-  int32_t* diffGrid;       // per view (tilesX+1)*(tilesY+1), cleared before
-  const uint32_t* gridBase;  // V offsets into diffGrid
+  int32_t* diffGrid;       // GRID_COPIES copies of: per view (tilesX+1)*(tilesY+1), cleared before
+  const uint32_t* gridBase;  // V offsets into a copy
+  uint32_t gridCells;      // cells of one copy (all views)
   float4* cullRecs;        // V * n warp-block cull parameters (p, q, kA, 0)
   uint4* itemSrc;          // V * n * 2: per visible slot (rect, mean, cull parameters, slot) for the expansion
 };
@@ -31,6 +39,7 @@ struct TileRangeArgs {
   const DevCam* cams;
   int32_t* diffGrid;
   const uint32_t* gridBase;
+  uint32_t gridCells;
   uint32_t* tileCnt;       // per global tile: the reference's tileCnt
   uint8_t* dropped;        // per global tile: dropped by the entry budget
   uint2* ranges;           // per global tile: [start, end) in the sorted entries

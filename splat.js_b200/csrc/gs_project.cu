@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(256, 4) k_project(ProjectArgs a) {  // 4 block
     a.itemSrc[2 * slot + 1] = make_uint4(__float_as_uint(cq.x), __float_as_uint(cq.y), __float_as_uint(cq.z),
                                          (uint32_t)slot);
     // rectangle add on the (tx+1) x (ty+1) difference grid
-    int32_t* gd = a.diffGrid + a.gridBase[v];
+    int32_t* gd = a.diffGrid + (size_t)(i & (GRID_COPIES - 1u)) * a.gridCells + a.gridBase[v];
     const int gw = tx + 1;
     atomicAdd(&gd[y0 * gw + x0], 1);
     atomicAdd(&gd[y0 * gw + x1 + 1], -1);
@@ -155,7 +155,11 @@ __global__ void __launch_bounds__(1024) k_tile_counts(TileRangeArgs a) {
     int32_t carry = 0;
     for (int x0 = 0; x0 < tx; x0 += 32) {
       const int x = x0 + lane;
-      int32_t v = x < tx ? gd[y * gw + x] : 0;
+      int32_t v = 0;
+      if (x < tx) {  // the copies' sum (order-free: integers)
+#pragma unroll
+        for (uint32_t k = 0; k < GRID_COPIES; ++k) v += gd[(size_t)k * a.gridCells + y * gw + x];
+      }
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
         const int32_t u = __shfl_up_sync(0xFFFFFFFFu, v, o);

@@ -406,7 +406,7 @@ int gs_setup(gs_trainer* h, const float* params, uint32_t n, const float* sh, co
   GS_AL(h->visList, (size_t)B * cap);
   GS_AL(h->gradP, (size_t)B * cap * GP_STRIDE);
   // (tx+1)(ty+1) = tiles + tx + ty + 1 <= 3 * maxTiles + 1 for any view of at most maxTiles tiles
-  GS_AL(h->diffGrid, (size_t)B * (3 * (size_t)h->maxTiles + 1));
+  GS_AL(h->diffGrid, (size_t)B * (3 * (size_t)h->maxTiles + 1) * GRID_COPIES);
   GS_AL(h->tileCnt, (size_t)B * h->maxTiles);
   GS_AL(h->dropped, (size_t)B * h->maxTiles);
   GS_AL(h->ranges, (size_t)B * h->maxTiles);
@@ -597,7 +597,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
     for (int k = 0; k < 5; ++k) cudaEventCreate(&ph[k]);
     cudaEventRecord(ph[0], s);
   }
-  cudaMemsetAsync(h->diffGrid, 0, (size_t)gridCells * 4, s);
+  cudaMemsetAsync(h->diffGrid, 0, (size_t)gridCells * GRID_COPIES * 4, s);
   cudaMemsetAsync(h->small, 0, 2057 * 4, s);  // hist, tile counters, work counter
   cudaMemsetAsync(h->small + 2062, 0, MAXB * 4, s);  // visible-item counters of the chain
   const uint64_t items = (uint64_t)sh.n * V;
@@ -617,6 +617,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   pa.pvals = h->pvals[0];
   pa.rect = h->rect;
   pa.diffGrid = h->diffGrid;
+  pa.gridCells = gridCells;
   pa.gridBase = h->dParams->gridBase;
   pa.cullRecs = h->cullRecs;
   pa.itemSrc = h->itemSrc;
@@ -626,6 +627,7 @@ static int enqueue_body(gs_trainer* h, const Shape& sh) {
   ta.V = V;
   ta.cams = dcams;
   ta.diffGrid = h->diffGrid;
+  ta.gridCells = gridCells;
   ta.gridBase = h->dParams->gridBase;
   ta.tileCnt = h->tileCnt;
   ta.dropped = h->dropped;
