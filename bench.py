@@ -60,6 +60,10 @@ def parse():
     ap.add_argument("--batch-depth", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--side-paths", action="store_true",
+                    help="measure the paths either side of the training step instead (the eval pass, PLY export "
+                         "with the opacity bake, frame undistortion), each through the C ABI beside the CPU "
+                         "restatement on the same inputs; prints one JSON line")
     ap.add_argument("--profile-window", action="store_true",
                     help="set up the workload, warm up, then run ONE batched step (tile 16, depth 256) between "
                          "cudaProfilerStart/Stop for ncu --profile-from-start off; prints no bench line")
@@ -489,8 +493,95 @@ def cpu_baseline_line(args, params, sh, cams):
                 "sample": f"failed: {e}"}
 
 
+def run_side_paths(args):
+    """The steps either side of the training path, on the headline scene: the
+    eval pass (_evalPass, trainer.js:542-574: a training-path pass without
+    Adam on one view, stats and camera gradients back), the PLY export with
+    the opacity bake over the 24 ring cameras (ply.js:17-99) and the frame
+    undistortion (undistortFrames, session.js:44-80) of eight 1080p frames.
+    Each is timed end to end through the C ABI (host buffers in and out, the
+    call returns when its results are in host memory), beside the oracle's
+    CPU restatement of the same step on the same inputs, all host threads."""
+    import torch
+    from oracle import oracle as O
+    from splat_b200 import native as N
+    from splat_b200 import scene
+    from splat_b200.session import cam_position, undistort_frames
+    from splat_b200.trainer import GSTrainer
+    O.build()
+    torch.cuda.set_device(0)
+    params, sh, cams = workload(args)
+    n = args.splats
+    opts = dict(shDeg=2, maxSplats=n, maxBatch=1, batchDepth=256, device=0, persistent=1, useGraphs=1)
+    pp, ps = scene.perturb(params, sh, 0.02, seed=args.seed + 1)
+    blank = [dict(tw=c["w"], th=c["h"], rgb=np.zeros(c["w"] * c["h"] * 3, np.float32)) for c in cams]
+    t = GSTrainer.create(opts)
+    t.setup(dict(data=pp, n=n, sh=ps), cams, blank, args.width, args.height, 4.0)
+    images = [dict(tw=c["w"], th=c["h"], rgb=np.ascontiguousarray(np.clip(t.renderView(c)[..., :3], 0, 1)
+                                                                  .reshape(-1))) for c in cams]
+    t.setup(dict(data=params, n=n, sh=sh), cams, images, args.width, args.height, 4.0)
+    del images, blank
+    t.iter = 2000
+    L, h = N.lib(), t._h
+    cores = O.set_threads(0)
+    out = {"workload": f"{n}-splat surface scene, SH 2, {args.width}x{args.height}", "cpu_threads": cores}
+
+    def wall(fn, reps):
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        return (time.perf_counter() - t0) / reps
+
+    # eval pass on camera 0
+    st = (C.c_uint32 * 4)()
+    cg = (C.c_int32 * ((len(cams) + 1) * 8))()
+    gpu_eval = wall(lambda: N.check(L.gs_eval_pass(h, 0, None, st, cg), h), 10)
+    o, ocams, targets = cpu_setup(args, params, sh, cams, 1)
+    p, s_ = params.copy(), sh.copy()
+    m, v = np.zeros_like(p), np.zeros_like(p)
+    sm, sv = np.zeros_like(s_), np.zeros_like(s_)
+    cpu_eval = wall(lambda: O.step(o, [ocams[0]], cpu_adam_hp(2001, 4.0), p, s_, targets, m, v, sm, sv, n,
+                                   do_adam=False), 1)
+    out["eval_pass"] = {"gpu_ms": gpu_eval * 1e3, "cpu_ms": cpu_eval * 1e3, "speedup": cpu_eval / gpu_eval,
+                        "what": "one 1080p view: project, bin, sort, raster forward + loss + backward, chain; "
+                                "stats and camera gradients read back"}
+    # PLY export with the opacity bake over the 24 ring cameras
+    campos = np.ascontiguousarray([cam_position(c) for c in cams], np.float64)
+    size = C.c_uint64()
+    N.check(L.gs_export_ply(h, 1, float(cams[0]["f"]), campos.ctypes.data_as(C.POINTER(C.c_double)),
+                            len(cams), None, 0, C.byref(size)), h)
+    buf = np.empty(size.value, np.uint8)
+    gpu_ply = wall(lambda: N.check(L.gs_export_ply(h, 1, float(cams[0]["f"]),
+                                                   campos.ctypes.data_as(C.POINTER(C.c_double)), len(cams),
+                                                   C.c_void_p(buf.ctypes.data), size.value, C.byref(size)), h), 5)
+    g = t.readGaussians()
+    cpu_ply = wall(lambda: O.ply_export(g["data"], g["n"], g["sh"], g["shK"], bake=True, f=float(cams[0]["f"]),
+                                        cam_positions=campos), 1)
+    out["ply_export"] = {"gpu_ms": gpu_ply * 1e3, "cpu_ms": cpu_ply * 1e3, "speedup": cpu_ply / gpu_ply,
+                         "bytes": int(size.value), "cameras": len(cams),
+                         "what": "bakeOpacityCompensation over the 24 cameras + gaussiansToPly, PLY bytes in "
+                                 "host memory (CPU: the numpy restatement of ply.js)"}
+    # undistortion of eight 1080p frames
+    rng = np.random.default_rng(args.seed + 7)
+    frames = [dict(tw=args.width, th=args.height, fw=float(args.width),
+                   rgb=rng.random(args.width * args.height * 3, dtype=np.float32)) for _ in range(8)]
+    recon = dict(k1=0.05, k2=-0.01, fFeat=1.17 * args.width)
+    gpu_und = wall(lambda: undistort_frames([dict(f) for f in frames], recon), 3)
+    cpu_und = wall(lambda: O.undistort_frames([dict(f) for f in frames], recon), 1)
+    out["undistort"] = {"gpu_ms": gpu_und * 1e3, "cpu_ms": cpu_und * 1e3, "speedup": cpu_und / gpu_und,
+                        "frames": len(frames), "bytes_each_way": len(frames) * args.width * args.height * 12,
+                        "what": "undistortFrames of 8 RGB float32 frames, k1 0.05, k2 -0.01, frames copied in "
+                                "and out (CPU: the numpy restatement of session.js)"}
+    out["clock"] = "host wall time around each call (the calls return with their results in host memory)"
+    print(json.dumps({"side_paths": out}), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.side_paths:
+        return run_side_paths(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

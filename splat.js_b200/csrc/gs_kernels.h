@@ -216,7 +216,8 @@ int onesweep_grid(int device);
 // staged through scratch (3 floats per pixel) on stream s.
 int pack_targets_device(const float* rgbHost, uint64_t np, float* scratch, uint32_t* out, cudaStream_t s);
 int export_ply_records(const float* params, const float* sh, uint32_t n, uint32_t K, int bake, double f,
-                       const double* camPosHost, uint32_t ncams, float* outHost, cudaStream_t s);
+                       const double* camPosHost, uint32_t ncams, double* dCam, float* dOut, void* outHost,
+                       cudaStream_t s);
 int debug_lookback_timeout(int device, uint32_t spinLimit, uint32_t* statusOut, double* msOut);
 void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s);
 void launch_raster(const RasterArgs& a, int mode, bool stored, int tile, int batchDepth, unsigned grid,

@@ -99,6 +99,11 @@ struct gs_trainer {
   uint64_t capacity = 0;
   uint32_t* small = nullptr;  // [0,2048) hist | [2048,2056) tileCounter | 2056 workCounter | 2057 totalEntries | 2058 scanTotal | 2059 epoch | 2060 status
   uint64_t* lbStatus = nullptr;
+  // PLY export scratch, grown on demand and kept: camera positions, records
+  double* plyCam = nullptr;
+  size_t plyCamCap = 0;
+  float* plyOut = nullptr;
+  size_t plyOutCap = 0;
   uint32_t* scanPartials = nullptr;
   float4* outImg = nullptr;
   float* finalT = nullptr;
@@ -199,6 +204,8 @@ static void free_all(gs_trainer* h) {
   h->allocs.clear();
   if (h->hRing) { cudaFreeHost(h->hRing); h->hRing = nullptr; }
   if (h->tStore) { cudaFree(h->tStore); h->tStore = nullptr; h->tStoreCap = 0; }
+  if (h->plyCam) { cudaFree(h->plyCam); h->plyCam = nullptr; h->plyCamCap = 0; }
+  if (h->plyOut) { cudaFree(h->plyOut); h->plyOut = nullptr; h->plyOutCap = 0; }
   h->rf = {};
   h->ready = false;
 }
@@ -983,12 +990,24 @@ int gs_export_ply(gs_trainer* h, int32_t bake, double f, const double* camPositi
   if (cap < *size) return fail(h, GS_E_LIMIT, "output buffer smaller than the PLY");
   cudaSetDevice(h->device);
   std::memcpy(out, hdr.data(), hdr.size());
-  std::vector<float> rec((size_t)h->n * (17 + 3 * h->K));
+  const size_t camBytes = bake && ncams ? (size_t)ncams * 3 * 8 : 8;
+  if (camBytes > h->plyCamCap) {
+    if (h->plyCam) cudaFree(h->plyCam);
+    h->plyCam = nullptr; h->plyCamCap = 0;
+    if (cudaMalloc(&h->plyCam, camBytes) != cudaSuccess) return fail(h, GS_E_NOMEM, "PLY export buffers");
+    h->plyCamCap = camBytes;
+  }
+  const size_t recBytes = body > 0 ? (size_t)body : 4;
+  if (recBytes > h->plyOutCap) {
+    if (h->plyOut) cudaFree(h->plyOut);
+    h->plyOut = nullptr; h->plyOutCap = 0;
+    if (cudaMalloc(&h->plyOut, recBytes) != cudaSuccess) return fail(h, GS_E_NOMEM, "PLY export buffers");
+    h->plyOutCap = recBytes;
+  }
+  // the records go from the device straight into the caller's buffer after the header
   const int rc = export_ply_records(h->params, h->K ? h->sh : nullptr, h->n, h->K, bake, f, camPositions, ncams,
-                                    rec.data(), h->stream);
-  if (rc == -3) return fail(h, GS_E_NOMEM, "PLY export buffers");
+                                    h->plyCam, h->plyOut, out + hdr.size(), h->stream);
   if (rc) return fail(h, GS_E_CUDA, "PLY export kernel");
-  std::memcpy(out + hdr.size(), rec.data(), body);
   return GS_OK;
 }
 
