@@ -119,6 +119,10 @@ export class GSTrainer {
   // readGaussians (trainer.js:797-817): {data, n, sh, shK}
   async readGaussians() { return addon.readGaussians(this.h); }
 
+  // no reference counterpart: the Adam moments back to setup()'s zeros, so a
+  // model written back trains on from a fresh optimiser state
+  resetMoments() { addon.resetMoments(this.h); }
+
   // renderView(camParams, target, trainMode, offset) (trainer.js:634-655): a
   // headless RGBA Float32Array replaces the canvas
   renderView(camParams, target = null, trainMode = 0, offset = 0) {

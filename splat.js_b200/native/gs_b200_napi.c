@@ -302,6 +302,18 @@ static napi_value set_u32(napi_env env, napi_callback_info info, int (*fn)(gs_tr
 }
 static napi_value SetIter(napi_env env, napi_callback_info info) { return set_u32(env, info, gs_set_iter); }
 static napi_value SetHorizon(napi_env env, napi_callback_info info) { return set_u32(env, info, gs_set_horizon); }
+/* resetMoments(h): Adam moments back to setup()'s zeros (no reference counterpart) */
+static napi_value ResetMoments(napi_env env, napi_callback_info info) {
+  size_t argc = 1;
+  napi_value argv[1];
+  NAPI_OK(env, napi_get_cb_info(env, info, &argc, argv, NULL, NULL));
+  Handle* H = arg_handle(env, argv[0]);
+  if (!H) return NULL;
+  pthread_mutex_lock(&H->mu);
+  const int rc = gs_reset_moments(H->h);
+  pthread_mutex_unlock(&H->mu);
+  return rc == GS_OK ? js_undefined(env) : throw_gs(env, H, rc);
+}
 static napi_value SetGrowLimit(napi_env env, napi_callback_info info) {
   return set_u32(env, info, gs_set_grow_limit);
 }
@@ -689,6 +701,7 @@ NAPI_MODULE_INIT() {
       {"renderView", RenderView}, {"evalPass", EvalPass},
       {"readCamGrads", ReadCamGrads}, {"refine", Refine},
       {"exportPly", ExportPly},   {"abiVersion", AbiVersion},
+      {"resetMoments", ResetMoments},
   };
   for (size_t k = 0; k < sizeof fns / sizeof fns[0]; ++k) {
     napi_value f;
